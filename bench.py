@@ -1,0 +1,320 @@
+"""Headline benchmark: exact triangle counting on an R-MAT scale-22 graph.
+
+Workload (one step = one triangle count of the whole graph):
+  R-MAT scale 22 (4,194,304 vertices), edge factor 16, (a,b,c,d) =
+  (0.57, 0.19, 0.19, 0.05), seeded (seed = 1 + rank), symmetrised, self-loops
+  and duplicates removed, int32 CSR with sorted lists, degree-oriented DAG
+  (ties by id).  Output: exact uint64 triangle count.
+Metric: TEPS = undirected edges / seconds per count (higher is better).
+
+  value    device-resident DAG in HBM, the count kernel(s) timed with CUDA
+           events on the launching stream (inputs 0.3 GB > 126 MB L2, so no
+           flush is needed between steps).
+  e2e      the same count through the C ABI from pinned HOST memory
+           (gpm_tc_host_csr: H2D of the symmetric CSR, orientation on the
+           device, count, D2H of the 8-byte result) -- all inside the timed
+           region.
+  roofline the count kernel against the measured HBM copy bandwidth, with
+           the algorithmic bytes B = 4(n+1) + 4m + 4*sum_{u->v} deg+(v).
+  cpu_baseline / --impl reference: the CPU restatement (OpenMP, all host
+           threads) timed on a bounded vertex sample of the same graph.
+
+Multi-GPU (torchrun): each rank counts its own independently seeded graph;
+no data-path collective (weak scaling); the timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpm-artifact_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+SCALE, EF = 22, 16
+A, B, C = 0.57, 0.19, 0.19
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (22 is the headline workload)")
+    ap.add_argument("--variant", default="auto", choices=["auto", "hash", "bsearch", "merge", "learned"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample time")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_sample(doff, didx, m_und, seconds, threads):
+    """Times the CPU restatement (OpenMP marker algorithm) on the tasks of a
+    vertex sample sized for about `seconds`, and scales to the whole graph by
+    the sample's share of the algorithmic work."""
+    import numpy as np
+    import _oracle as orc
+    n = len(doff) - 1
+    deg = np.diff(doff)
+    wv = np.zeros(n, np.float64)  # w(u) = d+(u) + sum_{v in N+(u)} d+(v)
+    np.add.at(wv, np.repeat(np.arange(n), deg), deg[didx].astype(np.float64))
+    wv += deg
+    total = wv.sum()
+
+    def run(stride):
+        keep = np.zeros(n, np.uint8)
+        keep[::stride] = 1
+        frac = wv[keep.astype(bool)].sum() / total
+        t0 = time.perf_counter()
+        orc.tc_tasks(doff, didx, keep, threads)
+        return time.perf_counter() - t0, frac
+
+    stride = 256
+    t, frac = run(stride)
+    while t < seconds / 3 and stride > 1:
+        stride = max(1, int(stride * max(0.05, t / seconds)))
+        t, frac = run(stride)
+    est_full = t / max(frac, 1e-12)
+    return m_und / est_full, (f"tasks of every {stride}-th vertex ({frac * 100:.2f}% of the wedge work) "
+                              f"in {t:.2f} s, scaled to the whole graph")
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import numpy as np
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world, dist)
+    import gpm
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    seed = 1 + rank
+    g = gpm.Graph.rmat(args.scale, EF, A, B, C, seed=seed)
+    sym_off, sym_idx = g.csr()
+    g.orient()
+    inf = g.info()
+    n, m_und = inf.n, inf.nnz
+    wedge, pair = g.work()
+    bytes_alg = 4 * (n + 1) + 4 * m_und + 4 * wedge
+    variant = {"auto": gpm.TC_AUTO, "hash": gpm.TC_HASH, "bsearch": gpm.TC_BSEARCH, "merge": gpm.TC_MERGE,
+               "learned": gpm.TC_LEARNED}[args.variant]
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    out = torch.zeros(1, dtype=torch.int64, device=dev)
+
+    for _ in range(max(args.warmup, 3)):
+        g.tc_async(variant, sp, out.data_ptr())
+    torch.cuda.synchronize()
+    count = int(out.item())
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record(stream)
+        for k in range(args.steps):
+            starts[k].record(stream)
+            g.tc_async(variant, sp, out.data_ptr())
+            ends[k].record(stream)
+        t_all1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms_total = t_all0.elapsed_time(t_all1)
+    per = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    assert int(out.item()) == count, "count changed between steps"
+    ms_step = ms_total / args.steps
+    if dist:
+        tt = torch.tensor([ms_step], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_step = float(tt.item())
+        me = torch.tensor([float(m_und)], device=dev)
+        dist.all_reduce(me, op=dist.ReduceOp.SUM)
+        m_total = float(me.item())
+    else:
+        m_total = float(m_und)
+    value = m_total / (ms_step / 1e3)
+
+    # ---- end to end through the C ABI from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        hoff = torch.from_numpy(sym_off).pin_memory()
+        hidx = torch.from_numpy(sym_idx).pin_memory()
+        nn = len(sym_off) - 1
+        for _ in range(2):
+            c2 = gpm.tc_host_csr_ptrs(nn, hoff.data_ptr(), hidx.data_ptr(), variant, sp)
+        assert c2 == count, (c2, count)
+        ks = max(3, min(args.steps, 5))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ks):
+            gpm.tc_host_csr_ptrs(nn, hoff.data_ptr(), hidx.data_ptr(), variant, sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1) / ks
+        if dist:
+            tt = torch.tensor([ms_e2e], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms_e2e = float(tt.item())
+        e2e = {"value": m_total / (ms_e2e / 1e3), "unit": "TEPS", "ms_per_step": ms_e2e,
+               "h2d_bytes_per_step": int(hoff.numel() * 8 + hidx.numel() * 4), "d2h_bytes_per_step": 8}
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        doff, didx = g.csr()
+        threads = len(os.sched_getaffinity(0))
+        v_cpu, sample = cpu_sample(doff, didx, m_und, args.cpu_seconds, threads)
+        cpu = {"value": v_cpu, "unit": "TEPS", "cores": threads, "kind": "port", "sample": sample}
+
+    hbm, peak_kind = peaks()
+    avg_kernel_ms = sum(per) / len(per)
+    achieved = bytes_alg / (avg_kernel_ms / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": "triangle-count TEPS (R-MAT scale 22, exact uint64)",
+            "value": value, "unit": "TEPS", "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int32", "data": "synthetic",
+            "config": {"workload": f"tc_rmat{args.scale}_ef{EF}", "graph": "R-MAT", "scale": args.scale,
+                       "edge_factor": EF, "abcd": [A, B, C, round(1 - A - B - C, 2)], "seed": "1+rank",
+                       "n": n, "m_undirected": m_und, "dag_max_outdeg": inf.max_degree,
+                       "triangles": count, "variant": args.variant, "parallelism": f"replicas{world}",
+                       "l2": "inputs > L2 (DAG %.0f MB), no flush" % ((8 * (n + 1) + 4 * m_und) / 1e6)},
+            "e2e": e2e,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": peak_kind,
+                         "traffic": None, "algorithmic_bytes": bytes_alg, "kernel_ms": avg_kernel_ms},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": args.steps * (1 if variant in (gpm.TC_AUTO, gpm.TC_HASH, gpm.TC_BSEARCH, gpm.TC_MERGE)
+                                          else 3),
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def reference_arm(args, rank, world, dist):
+    """The reference has no CPU triangle counter of its own; its arm is the
+    CPU restatement of its algorithm (oracle port) on all host threads."""
+    import numpy as np
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    import gpm
+    import _oracle as orc
+    n, s, d = gpm.gen_rmat(args.scale, EF, A, B, C, seed=1)
+    off, idx = orc.build_csr(n, s, d)
+    doff, didx = orc.orient(off, idx)
+    m_und = len(didx)
+    threads = len(os.sched_getaffinity(0))
+    vals = []
+    sample = ""
+    for k in range(max(args.warmup, 3) + args.steps):
+        v, sample = cpu_sample(doff, didx, m_und, min(args.cpu_seconds, 8.0), threads)
+        if k >= max(args.warmup, 3):
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"metric": "triangle-count TEPS (R-MAT scale 22, exact uint64)", "impl": "reference",
+            "value": value, "unit": "TEPS", "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": m_und / value * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": f"tc_rmat{args.scale}_ef{EF}", "graph": "R-MAT", "scale": args.scale,
+                       "edge_factor": EF, "parallelism": "cpu"},
+            "cpu_baseline": {"value": value, "unit": "TEPS", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "TEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

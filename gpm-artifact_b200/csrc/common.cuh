@@ -1,0 +1,180 @@
+// common.cuh -- shared definitions of libgpm: status/error plumbing, the
+// device graph handle, a counter-based RNG usable on host and device, and
+// warp helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "gpm.h"
+
+namespace gpm {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+int fail(int status, const std::string &msg);
+
+#define GPM_CUDA(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      return ::gpm::fail(e_ == cudaErrorMemoryAllocation ? GPM_ENOMEM : GPM_ECUDA, \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    }                                                                           \
+  } while (0)
+
+#define GPM_TRY(expr)            \
+  do {                           \
+    int s_ = (expr);             \
+    if (s_ != GPM_OK) return s_; \
+  } while (0)
+
+// Checks that a launch was accepted (configuration errors); execution errors
+// surface at the next synchronising call.
+#define GPM_LAUNCH_CHECK() GPM_CUDA(cudaGetLastError())
+
+int ensure_device();
+
+// ---------------------------------------------------------------- device buffers
+// Owning device allocation; move-only.
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) { reset(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  // Grows to at least count elements (contents not preserved).
+  int reserve(size_t count) {
+    if (count <= n && p) return GPM_OK;
+    reset();
+    size_t bytes = (count ? count : 1) * sizeof(T);
+    cudaError_t e = cudaMalloc((void **)&p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return fail(GPM_ENOMEM, "cudaMalloc(" + std::to_string(bytes) + " B) failed: " +
+                                  cudaGetErrorString(e));
+    }
+    n = count ? count : 1;
+    return GPM_OK;
+  }
+};
+
+// ---------------------------------------------------------------- RNG
+// splitmix64 finaliser: a counter-based generator, so edge i of a seeded
+// graph is the same whichever thread (host or device) draws it.
+__host__ __device__ inline uint64_t mix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__host__ __device__ inline uint64_t draw(uint64_t seed, uint64_t stream, uint64_t i) {
+  return mix64(mix64(seed ^ (stream * 0xD1B54A32D192ED03ull)) ^ i);
+}
+__host__ __device__ inline double unit(uint64_t r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
+// uniform integer in [0, n) for n < 2^32
+__host__ __device__ inline uint32_t below(uint64_t r, uint64_t n) {
+  return (uint32_t)(((r >> 32) * n) >> 32);
+}
+
+// R-MAT edge i: one quadrant draw per bit level, standard recursion.
+__host__ __device__ inline void rmat_edge(uint64_t seed, uint64_t i, int scale, double a, double b,
+                                          double c, int32_t *u, int32_t *v) {
+  uint32_t x = 0, y = 0;
+  const double ab = a + b, abc = a + b + c;
+  for (int l = 0; l < scale; ++l) {
+    double r = unit(draw(seed, 1 + l, i));
+    uint32_t bx = 0, by = 0;
+    if (r < a) {
+    } else if (r < ab) {
+      by = 1;
+    } else if (r < abc) {
+      bx = 1;
+    } else {
+      bx = 1;
+      by = 1;
+    }
+    x = (x << 1) | bx;
+    y = (y << 1) | by;
+  }
+  *u = (int32_t)x;
+  *v = (int32_t)y;
+}
+
+__host__ __device__ inline void er_edge(uint64_t seed, uint64_t i, int64_t n, int32_t *u, int32_t *v) {
+  *u = (int32_t)below(draw(seed, 101, i), (uint64_t)n);
+  *v = (int32_t)below(draw(seed, 102, i), (uint64_t)n);
+}
+
+// Chung-Lu endpoint: vertex index drawn with weight (i + i0)^(-alpha) by
+// inverting the continuous CDF of the weight profile.
+struct ChungLu {
+  double alpha, i0, lo, span, inv;  // lo = i0^(1-alpha), span = (n+i0)^(1-alpha) - lo
+  int64_t n;
+};
+__host__ __device__ inline int32_t chung_lu_vertex(const ChungLu &p, uint64_t r) {
+  double q = p.lo + unit(r) * p.span;
+  double x = pow(q, p.inv) - p.i0;
+  int64_t k = (int64_t)x;
+  if (k < 0) k = 0;
+  if (k >= p.n) k = p.n - 1;
+  return (int32_t)k;
+}
+ChungLu chung_lu_params(int64_t n, double gamma, double mean_deg);
+
+// ---------------------------------------------------------------- warp helpers
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------- graph handle
+struct TcPlan;
+struct MotifPlan;
+
+}  // namespace gpm
+
+struct gpm_graph {
+  int64_t n = 0;
+  int64_t nnz = 0;
+  int32_t max_deg = 0;
+  int oriented = 0;
+  int relabeled = 0;
+  int device = 0;
+  gpm::DevBuf<int64_t> off;     // n + 1
+  gpm::DevBuf<int32_t> adj;     // nnz
+  gpm::DevBuf<int32_t> labels;  // n (optional)
+  gpm::DevBuf<int32_t> src;     // nnz, COO source of each stored entry (lazy)
+  gpm::TcPlan *tc = nullptr;    // cached triangle-count schedule
+  gpm::DevBuf<uint64_t> result; // small device result scratch
+  ~gpm_graph();
+};
+
+namespace gpm {
+// graph.cu
+int build_csr_device(gpm_graph *g, int64_t n, int64_t m, const int32_t *d_src,
+                     const int32_t *d_dst, int symmetrize, cudaStream_t st);
+int ensure_src(gpm_graph *g, cudaStream_t st);
+int compute_max_degree(gpm_graph *g, cudaStream_t st);
+void free_tc_plan(TcPlan *p);
+int num_sms();
+}  // namespace gpm

@@ -1,0 +1,289 @@
+"""ctypes binding of libgpm.so (the C ABI declared in include/gpm.h).
+
+Tests and bench.py call the engine through this module, i.e. through the
+same extern "C" boundary a C, C++ or FFI caller uses.  Loading fails loudly
+when libgpm.so has not been built: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpm.so")
+
+GPM_OK = 0
+STATUS = {0: "GPM_OK", 1: "GPM_EINVAL", 2: "GPM_ECUDA", 3: "GPM_ENOMEM", 4: "GPM_EUNSUPPORTED",
+          5: "GPM_ETIMEOUT", 6: "GPM_EIO", 7: "GPM_ENODEV"}
+V_CENTRIC, E_CENTRIC = 0, 1
+TC_AUTO, TC_BSEARCH, TC_HASH, TC_MERGE, TC_LEARNED = 0, 1, 2, 3, 4
+G2MINER, PATTERN_SOLVER = 0, 1
+SYMMETRIZE = 1
+
+
+class GpmError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` "
+                          "(or __graft_entry__.build()); the engine has no CPU fallback")
+    return ctypes.CDLL(LIB_PATH)
+
+
+lib = _load()
+_P = c_void_p
+_SIGS = {
+    "gpm_last_error": ([], c_char_p),
+    "gpm_abi_version": ([], c_int),
+    "gpm_device_count": ([POINTER(c_int)], c_int),
+    "gpm_read_mtx": ([c_char_p, POINTER(c_int64), POINTER(c_int64), _P, _P, c_int64, POINTER(c_int32)], c_int),
+    "gpm_read_labels": ([c_char_p, c_int64, c_int32, _P], c_int),
+    "gpm_read_tve": ([c_char_p, POINTER(c_int64), POINTER(c_int64), _P, _P, _P, c_int64], c_int),
+    "gpm_gen_rmat": ([c_int, c_int, c_double, c_double, c_double, c_uint64, _P, _P], c_int),
+    "gpm_gen_er": ([c_int64, c_int64, c_uint64, _P, _P], c_int),
+    "gpm_gen_chung_lu": ([c_int64, c_double, c_double, c_uint64, POINTER(c_int64), _P, _P], c_int),
+    "gpm_gen_zipf_labels": ([c_int64, c_int, c_double, c_uint64, _P], c_int),
+    "gpm_graph_create": ([c_int64, c_int64, _P, _P, _P, c_int, POINTER(c_void_p)], c_int),
+    "gpm_graph_create_csr": ([c_int64, _P, _P, _P, POINTER(c_void_p)], c_int),
+    "gpm_graph_create_device": ([c_int64, c_int64, _P, _P, c_int, POINTER(c_void_p)], c_int),
+    "gpm_graph_generate": ([c_int, c_int64, c_int64, c_double, c_double, c_double, c_uint64,
+                            POINTER(c_void_p)], c_int),
+    "gpm_graph_destroy": ([_P], c_int),
+    "gpm_graph_get_info": ([_P, _P], c_int),
+    "gpm_graph_copy_csr": ([_P, _P, _P], c_int),
+    "gpm_graph_set_labels": ([_P, _P], c_int),
+    "gpm_graph_orient": ([_P, c_int], c_int),
+    "gpm_graph_work": ([_P, POINTER(c_uint64), POINTER(c_uint64)], c_int),
+    "gpm_tc": ([_P, c_int, POINTER(c_uint64)], c_int),
+    "gpm_tc_async": ([_P, c_int, _P, _P], c_int),
+    "gpm_tc_host_csr": ([c_int64, _P, _P, c_int, _P, POINTER(c_uint64)], c_int),
+    "gpm_clique": ([_P, c_int, POINTER(c_uint64)], c_int),
+    "gpm_motif": ([_P, c_int, _P], c_int),
+    "gpm_pattern": ([_P, c_char_p, c_int, _P, POINTER(c_uint64)], c_int),
+    "gpm_query_create": ([c_int64, c_int64, _P, _P, _P, POINTER(c_void_p)], c_int),
+    "gpm_query_destroy": ([_P], c_int),
+    "gpm_match": ([_P, _P, POINTER(c_uint64)], c_int),
+}
+for _name, (_args, _res) in _SIGS.items():
+    if hasattr(lib, _name):
+        _f = getattr(lib, _name)
+        _f.argtypes = _args
+        _f.restype = _res
+
+
+def check(status: int):
+    if status != GPM_OK:
+        raise GpmError(status, lib.gpm_last_error().decode(errors="replace"))
+
+
+def _ptr(a):
+    return None if a is None else c_void_p(a.ctypes.data)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class GraphInfo(ctypes.Structure):
+    _fields_ = [("n", c_int64), ("nnz", c_int64), ("max_degree", c_int32), ("oriented", c_int32),
+                ("relabeled", c_int32), ("has_labels", c_int32)]
+
+
+def device_count() -> int:
+    n = c_int(0)
+    check(lib.gpm_device_count(ctypes.byref(n)))
+    return n.value
+
+
+# ---------------------------------------------------------------- host helpers
+def read_mtx(path: str):
+    n, m, vmin = c_int64(), c_int64(), c_int32()
+    check(lib.gpm_read_mtx(path.encode(), ctypes.byref(n), ctypes.byref(m), None, None, 0, ctypes.byref(vmin)))
+    src = np.empty(m.value, np.int32)
+    dst = np.empty(m.value, np.int32)
+    check(lib.gpm_read_mtx(path.encode(), ctypes.byref(n), ctypes.byref(m), _ptr(src), _ptr(dst), m.value,
+                           ctypes.byref(vmin)))
+    return n.value, src, dst, vmin.value
+
+
+def read_labels(path: str, n: int, vmin: int = 0):
+    lab = np.empty(n, np.int32)
+    check(lib.gpm_read_labels(path.encode(), n, vmin, _ptr(lab)))
+    return lab
+
+
+def read_tve(path: str):
+    n, m = c_int64(), c_int64()
+    check(lib.gpm_read_tve(path.encode(), ctypes.byref(n), ctypes.byref(m), None, None, None, 0))
+    lab = np.empty(max(n.value, 1), np.int32)
+    src = np.empty(m.value, np.int32)
+    dst = np.empty(m.value, np.int32)
+    check(lib.gpm_read_tve(path.encode(), ctypes.byref(n), ctypes.byref(m), _ptr(lab), _ptr(src), _ptr(dst),
+                           m.value))
+    return n.value, src, dst, lab[: n.value]
+
+
+def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1):
+    m = (1 << scale) * edge_factor
+    src = np.empty(m, np.int32)
+    dst = np.empty(m, np.int32)
+    check(lib.gpm_gen_rmat(scale, edge_factor, a, b, c, seed, _ptr(src), _ptr(dst)))
+    return 1 << scale, src, dst
+
+
+def gen_er(n, m, seed=1):
+    src = np.empty(m, np.int32)
+    dst = np.empty(m, np.int32)
+    check(lib.gpm_gen_er(n, m, seed, _ptr(src), _ptr(dst)))
+    return n, src, dst
+
+
+def gen_chung_lu(n, gamma, mean_deg, seed=1):
+    m = c_int64()
+    check(lib.gpm_gen_chung_lu(n, gamma, mean_deg, seed, ctypes.byref(m), None, None))
+    src = np.empty(m.value, np.int32)
+    dst = np.empty(m.value, np.int32)
+    check(lib.gpm_gen_chung_lu(n, gamma, mean_deg, seed, ctypes.byref(m), _ptr(src), _ptr(dst)))
+    return n, src, dst
+
+
+def gen_zipf_labels(n, nlabels, s=1.2, seed=1):
+    lab = np.empty(n, np.int32)
+    check(lib.gpm_gen_zipf_labels(n, nlabels, s, seed, _ptr(lab)))
+    return lab
+
+
+# ---------------------------------------------------------------- device objects
+class Graph:
+    """Owning wrapper of a gpm_graph handle."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def from_edges(cls, n, src, dst, labels=None, symmetrize=True):
+        src, dst = _i32(src), _i32(dst)
+        lab = None if labels is None else _i32(labels)
+        h = c_void_p()
+        check(lib.gpm_graph_create(n, len(src), _ptr(src), _ptr(dst), _ptr(lab), SYMMETRIZE if symmetrize else 0,
+                                   ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_csr(cls, offsets, indices, labels=None):
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        idx = _i32(indices)
+        lab = None if labels is None else _i32(labels)
+        h = c_void_p()
+        check(lib.gpm_graph_create_csr(len(off) - 1, _ptr(off), _ptr(idx), _ptr(lab), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def generate(cls, kind, p0, p1=0, a=0.0, b=0.0, c=0.0, seed=1):
+        h = c_void_p()
+        check(lib.gpm_graph_generate(kind, p0, p1, a, b, c, seed, ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def rmat(cls, scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1):
+        return cls.generate(0, scale, edge_factor, a, b, c, seed)
+
+    def close(self):
+        if self.h:
+            lib.gpm_graph_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def info(self) -> GraphInfo:
+        inf = GraphInfo()
+        check(lib.gpm_graph_get_info(self.h, ctypes.byref(inf)))
+        return inf
+
+    def csr(self):
+        inf = self.info()
+        off = np.empty(inf.n + 1, np.int64)
+        idx = np.empty(max(inf.nnz, 1), np.int32)
+        check(lib.gpm_graph_copy_csr(self.h, _ptr(off), _ptr(idx)))
+        return off, idx[: inf.nnz]
+
+    def set_labels(self, labels):
+        lab = _i32(labels)
+        check(lib.gpm_graph_set_labels(self.h, _ptr(lab)))
+
+    def orient(self, relabel=False):
+        check(lib.gpm_graph_orient(self.h, 1 if relabel else 0))
+        return self
+
+    def work(self):
+        w, p = c_uint64(), c_uint64()
+        check(lib.gpm_graph_work(self.h, ctypes.byref(w), ctypes.byref(p)))
+        return w.value, p.value
+
+    def tc(self, mode=V_CENTRIC) -> int:
+        out = c_uint64()
+        check(lib.gpm_tc(self.h, mode, ctypes.byref(out)))
+        return out.value
+
+    def tc_async(self, variant, stream_ptr, d_out_ptr):
+        check(lib.gpm_tc_async(self.h, variant, c_void_p(stream_ptr), c_void_p(d_out_ptr)))
+
+    def clique(self, k) -> int:
+        out = c_uint64()
+        check(lib.gpm_clique(self.h, k, ctypes.byref(out)))
+        return out.value
+
+    def motif(self, k):
+        out = np.zeros(2 if k == 3 else 6, np.uint64)
+        check(lib.gpm_motif(self.h, k, _ptr(out)))
+        return out
+
+    def pattern(self, name, family=G2MINER):
+        counters = np.zeros(6, np.uint64)
+        res = c_uint64()
+        check(lib.gpm_pattern(self.h, name.encode(), family, _ptr(counters), ctypes.byref(res)))
+        return res.value, counters
+
+    def match(self, q: "Query") -> int:
+        out = c_uint64()
+        check(lib.gpm_match(self.h, q.h, ctypes.byref(out)))
+        return out.value
+
+
+class Query:
+    def __init__(self, n, src, dst, labels):
+        src, dst, lab = _i32(src), _i32(dst), _i32(labels)
+        h = c_void_p()
+        check(lib.gpm_query_create(n, len(src), _ptr(src), _ptr(dst), _ptr(lab), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.gpm_query_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+
+def tc_host_csr(offsets, indices, variant=TC_AUTO, stream_ptr=0) -> int:
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    idx = _i32(indices)
+    out = c_uint64()
+    check(lib.gpm_tc_host_csr(len(off) - 1, _ptr(off), _ptr(idx), variant, c_void_p(stream_ptr),
+                              ctypes.byref(out)))
+    return out.value
+
+
+def tc_host_csr_ptrs(n, off_ptr, idx_ptr, variant, stream_ptr) -> int:
+    """Same as tc_host_csr on raw (pinned) host pointers."""
+    out = c_uint64()
+    check(lib.gpm_tc_host_csr(n, c_void_p(off_ptr), c_void_p(idx_ptr), variant, c_void_p(stream_ptr),
+                              ctypes.byref(out)))
+    return out.value

@@ -1,0 +1,195 @@
+/*
+ * gpm.h -- C ABI of the B200 graph-pattern-mining count engine (libgpm.so).
+ *
+ * This boundary replaces the header-only template solvers of the AntiRF
+ * reference (namespace project_AntiRF).  Each entry point below names the
+ * reference interface it stands in for.  Conventions:
+ *   - every function returns a gpm_status (0 = GPM_OK); nothing aborts.
+ *     gpm_last_error() gives the message of the calling thread's last error;
+ *   - host buffers are caller-owned; device memory owned by a handle is
+ *     freed by its *_destroy;
+ *   - counts are exact uint64 (the reference's AccType, src/utils/utils.h:25);
+ *   - neighbour lists are kept sorted ascending and duplicate-free (the
+ *     reference's binary searches, src/graph/search.cuh:20-87, are only
+ *     defined on such lists);
+ *   - "stream" arguments are a cudaStream_t passed as void* (NULL = the
+ *     legacy default stream).  Synchronous calls block on that stream.
+ */
+#ifndef GPM_H
+#define GPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPM_ABI_VERSION 1
+
+typedef enum {
+  GPM_OK = 0,
+  GPM_EINVAL = 1,       /* bad argument (also: unknown pattern name)          */
+  GPM_ECUDA = 2,        /* CUDA runtime error                                 */
+  GPM_ENOMEM = 3,       /* device or host allocation failed                   */
+  GPM_EUNSUPPORTED = 4, /* request outside what the engine implements         */
+  GPM_ETIMEOUT = 5,     /* a device watchdog ended a kernel early             */
+  GPM_EIO = 6,          /* file could not be opened or parsed                 */
+  GPM_ENODEV = 7        /* no CUDA device                                     */
+} gpm_status;
+
+/* src/utils/utils.h:24  enum modes {v_centric, e_centric} */
+enum { GPM_V_CENTRIC = 0, GPM_E_CENTRIC = 1 };
+
+/* Triangle-count kernel variants (all return the same count). */
+enum {
+  GPM_TC_AUTO = 0,     /* engine's choice: learned scheduler if trained, else heuristic */
+  GPM_TC_BSEARCH = 1,  /* warp per stored edge, binary search (TCSolver.cuh:27-59 shape) */
+  GPM_TC_HASH = 2,     /* vertex tasks, shared-memory hash of N(u), hub/tail queues
+                          with the fixed thresholds of tuning_schedules.cuh:196-197   */
+  GPM_TC_MERGE = 3,    /* warp per stored edge, merge-path intersection             */
+  GPM_TC_LEARNED = 4   /* per-task variant and split chosen by the MLP cost model   */
+};
+
+/* Pattern families: G2MinerSolver (src/G2MinerSolver.cuh) and PatternSolver
+ * (src/PatternSolver.cuh). */
+enum { GPM_G2MINER = 0, GPM_PATTERN_SOLVER = 1 };
+
+/* Graph-construction flags for gpm_graph_create. */
+enum {
+  GPM_SYMMETRIZE = 1  /* add v->u for every u->v (undirected input) */
+};
+
+typedef struct gpm_graph gpm_graph;
+typedef struct gpm_query gpm_query;
+
+typedef struct {
+  int64_t n;           /* vertices                                  */
+  int64_t nnz;         /* stored directed entries                   */
+  int32_t max_degree;  /* max stored out-degree                     */
+  int32_t oriented;    /* 1 after gpm_graph_orient                   */
+  int32_t relabeled;   /* 1 if orient() also relabelled by degree    */
+  int32_t has_labels;  /* vertex labels present                      */
+} gpm_graph_info;
+
+/* ---- errors / device --------------------------------------------------- */
+const char *gpm_last_error(void);
+int gpm_abi_version(void);
+/* Number of visible CUDA devices (0 when none). */
+int gpm_device_count(int *count);
+
+/* ---- file formats (host only, no device needed) ------------------------- */
+/* Loader::_load_mtx, src/graph/io.h:84-139: skip '%' comment lines, read the
+ * "n n m" header, drop self-loops, shift ids by the minimum id.  Two-call
+ * pattern: with src == NULL only *n and *m are returned.  *vmin receives the
+ * id shift (needed by gpm_read_labels). */
+int gpm_read_mtx(const char *path, int64_t *n, int64_t *m, int32_t *src, int32_t *dst,
+                 int64_t cap, int32_t *vmin);
+/* Loader::LoadVLabel, src/graph/io.h:35-73: "v label" lines (v shifted by
+ * vmin) or the literal "random<N>" (labels rand() % N with the C library's
+ * rand(), as the reference does). */
+int gpm_read_labels(const char *path, int64_t n, int32_t vmin, int32_t *labels);
+/* sub_ceci Graph::loadGraphFromFile (sub_ceci/graph/graph.cpp:86-166) "t/v/e"
+ * format, and the querysets "t # 0 / v id label / e u v elabel" format.
+ * Two-call pattern as above.  Edges are returned as listed (once each). */
+int gpm_read_tve(const char *path, int64_t *n, int64_t *m, int32_t *labels, int32_t *src,
+                 int32_t *dst, int64_t cap);
+
+/* ---- seeded synthetic generators (host, OpenMP; identical on device) ------ */
+/* R-MAT: scale, edge_factor * 2^scale draws, quadrant probabilities a,b,c. */
+int gpm_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                 int32_t *src, int32_t *dst);
+/* Erdos-Renyi G(n, m draws): uniform endpoints. */
+int gpm_gen_er(int64_t n, int64_t m, uint64_t seed, int32_t *src, int32_t *dst);
+/* Chung-Lu: expected degrees w_i ~ (i+i0)^(-1/(gamma-1)) scaled to mean
+ * degree mean_deg; m = round(n * mean_deg / 2) draws. Returns *m first when
+ * src == NULL. */
+int gpm_gen_chung_lu(int64_t n, double gamma, double mean_deg, uint64_t seed, int64_t *m,
+                     int32_t *src, int32_t *dst);
+/* Zipf(s) labels in [0, nlabels). */
+int gpm_gen_zipf_labels(int64_t n, int nlabels, double s, uint64_t seed, int32_t *labels);
+
+/* ---- graphs ---------------------------------------------------------------- */
+/* Loader::Build + Graph::Init (src/graph/io.h:75-81, src/graph/graph.h:254-340):
+ * builds the device CSR from a host edge list.  Self-loops and duplicate
+ * entries are dropped and every list is sorted (Init keeps input order; the
+ * reference kernels need sorted lists).  labels may be NULL. */
+int gpm_graph_create(int64_t n, int64_t m, const int32_t *src, const int32_t *dst,
+                     const int32_t *labels, int flags, gpm_graph **out);
+/* Same, from a host CSR that is already sorted and duplicate-free
+ * (offsets[n+1], indices[offsets[n]]). Validated on the device. */
+int gpm_graph_create_csr(int64_t n, const int64_t *offsets, const int32_t *indices,
+                         const int32_t *labels, gpm_graph **out);
+/* Build a graph whose edge list already lives in device memory. */
+int gpm_graph_create_device(int64_t n, int64_t m, const int32_t *d_src, const int32_t *d_dst,
+                            int flags, gpm_graph **out);
+/* Seeded R-MAT / ER / Chung-Lu graph generated and built on the device
+ * (symmetrised, simple).  kind: 0 = R-MAT(p0=scale, p1=edge factor, a,b,c),
+ * 1 = ER(p0=n, p1=m draws), 2 = Chung-Lu(p0=n, a=gamma, b=mean degree). */
+int gpm_graph_generate(int kind, int64_t p0, int64_t p1, double a, double b, double c,
+                       uint64_t seed, gpm_graph **out);
+int gpm_graph_destroy(gpm_graph *g);
+int gpm_graph_get_info(const gpm_graph *g, gpm_graph_info *info);
+/* Copy the device CSR to caller buffers (offsets[n+1], indices[nnz]). */
+int gpm_graph_copy_csr(const gpm_graph *g, int64_t *offsets, int32_t *indices);
+int gpm_graph_set_labels(gpm_graph *g, const int32_t *labels);
+/* Graph::orientation (graph.h:116-204): keep u->v iff d(v) > d(u) or
+ * (d(v) == d(u) and v > u).  relabel != 0 additionally applies
+ * Graph::SortCSRGraph (graph.h:206-252): vertices renumbered by out-degree
+ * descending (stable), lists re-sorted.  Runs on the device. */
+int gpm_graph_orient(gpm_graph *g, int relabel);
+/* Algorithmic work figures of the (oriented) graph: *wedge_work =
+ * sum over stored u->v of deg(v); *pair_work = sum over u->v of
+ * (deg(u) + deg(v)). */
+int gpm_graph_work(gpm_graph *g, uint64_t *wedge_work, uint64_t *pair_work);
+
+/* ---- counting ---------------------------------------------------------------- */
+/* TCSolver (src/TCSolver.cuh:9-121): sum over stored edges u->v of
+ * |N(u) & N(v)|.  On an oriented graph this is the triangle count (the
+ * reference's Engine::RunTC orients first, src/Engine.h:47-56).
+ * mode: GPM_V_CENTRIC / GPM_E_CENTRIC choose the default variant
+ * (GPM_TC_HASH / GPM_TC_BSEARCH) when variant == GPM_TC_AUTO and no trained
+ * scheduler is attached. */
+int gpm_tc(gpm_graph *g, int mode, uint64_t *out);
+/* Explicit variant, asynchronous: writes the count to device memory d_out
+ * (8 bytes) on stream; no host synchronisation; capturable. */
+int gpm_tc_async(gpm_graph *g, int variant, void *stream, uint64_t *d_out);
+/* End to end from host memory: upload a symmetric CSR (sorted,
+ * duplicate-free), orient on the device, count, return the count.  This is
+ * the RunTC path as one call.  stream may be NULL. */
+int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, int variant,
+                    void *stream, uint64_t *out);
+
+/* CFSolver (src/CFSolver.cuh:99-158): k-clique count on an oriented graph,
+ * k in [3, 8]. */
+int gpm_clique(gpm_graph *g, int k, uint64_t *out);
+
+/* Motif counting on a symmetric graph.  k = 3: out[0] = induced 2-paths,
+ * out[1] = triangles.  k = 4: out[0..5] = 3-star, 4-path, tailed triangle,
+ * 4-cycle, diamond, 4-clique -- the counter order of Motif4_G2Miner
+ * (src/gpu_kernels/G2Miner_kernels.cuh:473-548). */
+int gpm_motif(gpm_graph *g, int k, uint64_t *out);
+
+/* G2MinerSolver / PatternSolver (src/G2MinerSolver.cuh:17-176,
+ * src/PatternSolver.cuh:16-265) on a symmetric graph.  name: "P1".."P8" or
+ * "Motif4".  counters (may be NULL) receive the solver's 6-entry counter
+ * array; *result the value the solver returns (h_total[0] for G2Miner,
+ * h_total[1] or h_total[1]-h_total[2] for PatternSolver). */
+int gpm_pattern(gpm_graph *g, const char *name, int family, uint64_t *counters,
+                uint64_t *result);
+
+/* ---- labelled subgraph matching (sub_ceci semantics) ----------------------- */
+/* Query graph: n vertices (n <= 16), m undirected edges listed once, labels. */
+int gpm_query_create(int64_t n, int64_t m, const int32_t *src, const int32_t *dst,
+                     const int32_t *labels, gpm_query **out);
+int gpm_query_destroy(gpm_query *q);
+/* Number of injective, label-preserving maps of the query into the data
+ * graph that send every query edge to a data edge (sub_ceci/myceci.cpp:540-668
+ * counts the same embeddings).  The data graph must be symmetric and carry
+ * labels. */
+int gpm_match(gpm_graph *data, const gpm_query *q, uint64_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPM_H */

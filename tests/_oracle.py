@@ -1,0 +1,108 @@
+"""ctypes binding of oracle/liboracle.so -- the CPU checker (test infrastructure).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import c_int, c_int64, c_uint64, c_void_p
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            raise ImportError(f"{ORACLE_SO} missing: run `make -C {os.path.dirname(ORACLE_SO)}`")
+        L = ctypes.CDLL(ORACLE_SO)
+        for f in ("orc_tc", "orc_tc_tasks", "orc_tc_merge", "orc_clique", "orc_pattern_g2miner", "orc_pattern_solver", "orc_match"):
+            getattr(L, f).restype = c_uint64
+        L.orc_build_csr.restype = c_int64
+        L.orc_orient.restype = c_int64
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return c_void_p(a.ctypes.data)
+
+
+def build_csr(n, src, dst, symmetrize=True):
+    s0 = np.ascontiguousarray(src, np.int32)
+    s1 = np.ascontiguousarray(dst, np.int32)
+    off = np.zeros(n + 1, np.int64)
+    idx = np.zeros(2 * len(s0) + 1, np.int32)
+    m = lib().orc_build_csr(c_int64(n), c_int64(len(s0)), _p(s0), _p(s1), 1 if symmetrize else 0, _p(off),
+                            _p(idx), c_int64(len(idx)))
+    assert m >= 0
+    return off, idx[:m].copy()
+
+
+def orient(off, idx):
+    n = len(off) - 1
+    off = np.ascontiguousarray(off, np.int64)
+    idx = np.ascontiguousarray(idx, np.int32)
+    doff = np.zeros(n + 1, np.int64)
+    didx = np.zeros(len(idx) + 1, np.int32)
+    m = lib().orc_orient(c_int64(n), _p(off), _p(idx), _p(doff), _p(didx))
+    return doff, didx[:m].copy()
+
+
+def tc(doff, didx, threads=0):
+    return lib().orc_tc(c_int64(len(doff) - 1), _p(doff), _p(didx), c_int(threads))
+
+
+def tc_tasks(doff, didx, keep, threads=0):
+    keep = np.ascontiguousarray(keep, np.uint8)
+    return lib().orc_tc_tasks(c_int64(len(doff) - 1), _p(doff), _p(didx), _p(keep), c_int(threads))
+
+
+def tc_merge(doff, didx):
+    return lib().orc_tc_merge(c_int64(len(doff) - 1), _p(doff), _p(didx))
+
+
+def clique(doff, didx, k, threads=0):
+    return lib().orc_clique(c_int64(len(doff) - 1), _p(doff), _p(didx), c_int(k), c_int(threads))
+
+
+def motif4(off, idx, threads=0):
+    out = (c_uint64 * 6)()
+    lib().orc_motif4_g2miner(c_int64(len(off) - 1), _p(off), _p(idx), out, c_int(threads))
+    return np.array(list(out), np.uint64)
+
+
+def bruteforce(off, idx):
+    out = (c_uint64 * 8)()
+    lib().orc_motif_bruteforce(c_int64(len(off) - 1), _p(off), _p(idx), out)
+    return np.array(list(out), np.uint64)
+
+
+def pattern_g2miner(off, idx, p, threads=0):
+    return lib().orc_pattern_g2miner(c_int64(len(off) - 1), _p(off), _p(idx), c_int(p), c_int(threads))
+
+
+def pattern_solver(off, idx, p, threads=0):
+    out = (c_uint64 * 6)()
+    r = lib().orc_pattern_solver(c_int64(len(off) - 1), _p(off), _p(idx), c_int(p), out, c_int(threads))
+    return r, np.array(list(out), np.uint64)
+
+
+def match(off, idx, labels, qoff, qidx, qlabels, threads=0):
+    labels = np.ascontiguousarray(labels, np.int32)
+    qlabels = np.ascontiguousarray(qlabels, np.int32)
+    return lib().orc_match(c_int64(len(off) - 1), _p(off), _p(idx), _p(labels), c_int64(len(qoff) - 1), _p(qoff),
+                           _p(qidx), _p(qlabels), c_int(threads))
+
+
+def motif3(off, idx, tri):
+    """3-vertex motifs: induced 2-paths = sum C(d,2) - 3T, triangles."""
+    d = np.diff(off).astype(np.uint64)
+    wedges = int(np.sum(d * (d - np.uint64(1)) // np.uint64(2))) if len(d) else 0
+    return np.array([wedges - 3 * tri, tri], np.uint64)
