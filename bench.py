@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (22 is the headline workload)")
-    ap.add_argument("--variant", default="auto", choices=["auto", "hash", "bsearch", "merge", "learned"])
+    ap.add_argument("--variant", default="auto", choices=["auto", "bitmap", "hash", "bsearch", "merge", "learned"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample time")
@@ -173,7 +173,7 @@ def main():
     n, m_und = inf.n, inf.nnz
     wedge, pair = g.work()
     bytes_alg = 4 * (n + 1) + 4 * m_und + 4 * wedge
-    variant = {"auto": gpm.TC_AUTO, "hash": gpm.TC_HASH, "bsearch": gpm.TC_BSEARCH, "merge": gpm.TC_MERGE,
+    variant = {"auto": gpm.TC_AUTO, "bitmap": gpm.TC_BITMAP, "hash": gpm.TC_HASH, "bsearch": gpm.TC_BSEARCH, "merge": gpm.TC_MERGE,
                "learned": gpm.TC_LEARNED}[args.variant]
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream

@@ -149,6 +149,7 @@ __device__ __forceinline__ T warp_sum(T v) {
 
 // ---------------------------------------------------------------- graph handle
 struct TcPlan;
+struct RankPlan;
 struct MotifPlan;
 
 }  // namespace gpm
@@ -164,7 +165,8 @@ struct gpm_graph {
   gpm::DevBuf<int32_t> adj;     // nnz
   gpm::DevBuf<int32_t> labels;  // n (optional)
   gpm::DevBuf<int32_t> src;     // nnz, COO source of each stored entry (lazy)
-  gpm::TcPlan *tc = nullptr;    // cached triangle-count schedule
+  gpm::TcPlan *tc = nullptr;    // cached triangle-count schedule (HASH)
+  gpm::RankPlan *rank = nullptr; // cached schedule of the BITMAP path
   gpm::DevBuf<uint64_t> result; // small device result scratch
   ~gpm_graph();
 };
@@ -176,5 +178,6 @@ int build_csr_device(gpm_graph *g, int64_t n, int64_t m, const int32_t *d_src,
 int ensure_src(gpm_graph *g, cudaStream_t st);
 int compute_max_degree(gpm_graph *g, cudaStream_t st);
 void free_tc_plan(TcPlan *p);
+void free_rank_plan(RankPlan *p);
 int num_sms();
 }  // namespace gpm

@@ -377,7 +377,10 @@ __global__ void k_work(int64_t n, const int64_t *__restrict__ off, const int32_t
 
 using namespace gpm;
 
-gpm_graph::~gpm_graph() { free_tc_plan(tc); }
+gpm_graph::~gpm_graph() {
+  free_tc_plan(tc);
+  free_rank_plan(rank);
+}
 
 extern "C" {
 
@@ -543,6 +546,8 @@ int gpm_graph_orient(gpm_graph *g, int relabel) {
   if (!g) return fail(GPM_EINVAL, "NULL graph");
   free_tc_plan(g->tc);
   g->tc = nullptr;
+  free_rank_plan(g->rank);
+  g->rank = nullptr;
   GPM_TRY(orient_on_stream(g, 0));
   if (relabel) GPM_TRY(relabel_device(g, 0));
   GPM_TRY(compute_max_degree(g, 0));

@@ -20,6 +20,7 @@
 
 #include "common.cuh"
 #include "tc.cuh"
+#include "tc_rank.cuh"
 
 namespace gpm {
 
@@ -388,6 +389,7 @@ int tc_launch(gpm_graph *g, int variant, cudaStream_t st, unsigned long long *d_
     GPM_LAUNCH_CHECK();
     return GPM_OK;
   }
+  if (variant == GPM_TC_BITMAP) return rank_launch(g, st, d_out);
   return fail(GPM_EINVAL, "unknown triangle-count variant " + std::to_string(variant));
 }
 
@@ -399,7 +401,7 @@ extern "C" {
 
 int gpm_tc_async(gpm_graph *g, int variant, void *stream, uint64_t *d_out) {
   if (!g || !d_out) return fail(GPM_EINVAL, "gpm_tc_async: NULL argument");
-  if (variant == GPM_TC_AUTO) variant = GPM_TC_HASH;
+  if (variant == GPM_TC_AUTO) variant = GPM_TC_BITMAP;
   if (variant == GPM_TC_LEARNED) return tc_learned_launch(g, (cudaStream_t)stream, (unsigned long long *)d_out);
   return tc_launch(g, variant, (cudaStream_t)stream, (unsigned long long *)d_out);
 }
@@ -429,7 +431,7 @@ int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, i
   if (nnz > 0) GPM_CUDA(cudaMemcpyAsync(g.adj.p, indices, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
   GPM_TRY(orient_on_stream(&g, st));
   GPM_TRY(g.result.reserve(8));
-  if (variant == GPM_TC_AUTO) variant = GPM_TC_HASH;
+  if (variant == GPM_TC_AUTO) variant = GPM_TC_BITMAP;
   if (variant == GPM_TC_LEARNED) GPM_TRY(tc_learned_launch(&g, st, (unsigned long long *)g.result.p));
   else GPM_TRY(tc_launch(&g, variant, st, (unsigned long long *)g.result.p));
   GPM_CUDA(cudaMemcpyAsync(out, g.result.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));

@@ -1,0 +1,483 @@
+// tc_rank.cu -- the B200 triangle-count path (variant GPM_TC_BITMAP).
+//
+// Same sum as every TCSolver variant, T = sum over stored u->v of
+// |N(u) & N(v)|, reorganised three ways:
+//
+// 1. Rank relabel.  Vertices are renumbered by (in+out degree, id), the
+//    order the degree orientation (graph.h:128-129) is built on, so a DAG
+//    edge always points to a larger id and the out-list of a high-degree
+//    vertex is a short run of large ids.
+// 2. Smaller side probes.  Each stored edge is owned by the endpoint with
+//    the longer list ("owner"); the other endpoint is its "partner".  An
+//    owner task loads N(owner) once and streams the lists N(partner) of all
+//    its partners.  The streamed work is sum over edges of
+//    min(d(u), d(v)) instead of sum d(v) (2.3x less on R-MAT).
+// 3. Direct-mapped bitmap.  After the relabel nearly every owner list spans
+//    fewer than 2^17 ids, so membership is one shared-memory bit test (no
+//    hashing, no probe loops, no divergence).  Owners whose span is wider
+//    fall back to an open-addressing table.
+//
+// Long partner lists are streamed by a whole warp with 16-byte vector loads;
+// short ones by 8-lane groups.  Owners with more than `cta_min` keys are CTA
+// tasks, the rest warp tasks; both queues are sorted heaviest first and
+// drained by a persistent grid.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "tc.cuh"
+#include "tc_rank.cuh"
+
+namespace gpm {
+
+constexpr int kRWarps = 8;
+constexpr int kCtaWords = 4096;        // 16 KB: bitmap of 2^17 bits or 4096 hash slots
+constexpr int kWarpWords = 512;        // 2 KB per warp: 2^14 bits or 512 hash slots
+constexpr int kCtaHashChunk = 2048;    // keys per hash chunk (load <= 0.5)
+constexpr int kWarpHashChunk = 256;
+static_assert(kWarpWords * kRWarps == kCtaWords, "warp regions tile the CTA region");
+constexpr size_t kRankSmem = kCtaWords * 4;
+
+static int grid_for(int64_t work, int block = 256) {
+  int64_t g = (work + block - 1) / block;
+  int64_t cap = (int64_t)num_sms() * 16;
+  return (int)std::max<int64_t>(1, std::min(g, cap));
+}
+
+// ------------------------------------------------------------ membership
+struct BitTable {
+  const uint32_t *bm;
+  int32_t base;
+  uint32_t span;
+  __device__ __forceinline__ unsigned hit(int32_t w) const {
+    uint32_t o = (uint32_t)(w - base);
+    return o < span ? (bm[o >> 5] >> (o & 31)) & 1u : 0u;
+  }
+};
+struct HashTable {
+  const int32_t *tab;
+  int logcap;
+  __device__ __forceinline__ unsigned hit(int32_t w) const {
+    uint32_t mask = (1u << logcap) - 1u;
+    uint32_t h = ((uint32_t)w * 2654435769u) >> (32 - logcap);
+    while (true) {
+      int32_t k = tab[h];
+      if (k == w) return 1u;
+      if (k < 0) return 0u;
+      h = (h + 1) & mask;
+    }
+  }
+};
+
+// Stream one sorted list [s, e) with the whole warp: 16-byte loads for the
+// aligned body, scalar loads for the unaligned head and tail.
+template <class T>
+__device__ __forceinline__ unsigned long long warp_stream(const int32_t *__restrict__ adj, int64_t s,
+                                                          int64_t e, const T &t, unsigned lane) {
+  unsigned long long c = 0;
+  int64_t a = min((s + 3) & ~(int64_t)3, e);
+  if ((int64_t)lane < a - s) c += t.hit(__ldg(adj + s + lane));
+  int64_t nv = (e - a) >> 2;
+  const int4 *p = reinterpret_cast<const int4 *>(adj + a);
+#pragma unroll 2
+  for (int64_t i = lane; i < nv; i += 32) {
+    int4 q = __ldg(p + i);
+    c += t.hit(q.x) + t.hit(q.y) + t.hit(q.z) + t.hit(q.w);
+  }
+  int64_t tl = a + nv * 4;
+  if ((int64_t)lane < e - tl) c += t.hit(__ldg(adj + tl + lane));
+  return c;
+}
+
+// Partners [p0, p1) of one owner: the first nlong are long lists (whole
+// warp each), the rest short (8-lane groups).  `wid`/`nw` spread partners
+// over the warps of the executing group (1 warp for warp tasks, the CTA's
+// warps for CTA tasks).
+template <class T>
+__device__ __forceinline__ unsigned long long scan_partners(const int64_t *__restrict__ roff,
+                                                            const int32_t *__restrict__ radj,
+                                                            const int32_t *__restrict__ padj, int64_t p0,
+                                                            int64_t p1, int nlong, const T &t, int wid,
+                                                            int nw, unsigned lane) {
+  unsigned long long c = 0;
+  for (int64_t j = p0 + wid; j < p0 + nlong; j += nw) {
+    int32_t y = padj[j];
+    c += warp_stream(radj, roff[y], roff[y + 1], t, lane);
+  }
+  const unsigned grp = lane >> 3, gl = lane & 7;
+  for (int64_t j = p0 + nlong + wid * 4 + grp; j < p1; j += nw * 4) {
+    int32_t y = padj[j];
+    int64_t s = roff[y], e = roff[y + 1];
+    for (int64_t k = s + gl; k < e; k += 8) c += t.hit(__ldg(radj + k));
+  }
+  return c;
+}
+
+__device__ __forceinline__ int ceil_log2i(int x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
+
+// ------------------------------------------------------------ tasks
+__device__ unsigned long long rank_cta_task(int32_t x, const int64_t *__restrict__ roff,
+                                            const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
+                                            const int32_t *__restrict__ padj, const int32_t *__restrict__ plong,
+                                            uint32_t *words) {
+  const int tid = threadIdx.x, nthr = blockDim.x, wid = tid >> 5, nw = nthr >> 5;
+  const unsigned lane = tid & 31;
+  const int64_t s0 = roff[x];
+  const int d = (int)(roff[x + 1] - s0);
+  const int64_t p0 = poff[x], p1 = poff[x + 1];
+  const int nl = plong[x];
+  const int32_t kmin = radj[s0], kmax = radj[s0 + d - 1];
+  const int64_t span = (int64_t)kmax - kmin + 1;
+  unsigned long long c = 0;
+  if (span <= (int64_t)kCtaWords * 32) {
+    const int nwords = (int)((span + 31) >> 5);
+    for (int i = tid; i < nwords; i += nthr) words[i] = 0u;
+    __syncthreads();
+    for (int i = tid; i < d; i += nthr) {
+      uint32_t o = (uint32_t)(radj[s0 + i] - kmin);
+      atomicOr(&words[o >> 5], 1u << (o & 31));
+    }
+    __syncthreads();
+    BitTable t{words, kmin, (uint32_t)span};
+    c = scan_partners(roff, radj, padj, p0, p1, nl, t, wid, nw, lane);
+  } else {
+    int32_t *tab = reinterpret_cast<int32_t *>(words);
+    for (int t0 = 0; t0 < d; t0 += kCtaHashChunk) {
+      const int tk = min(kCtaHashChunk, d - t0);
+      const int logcap = max(5, ceil_log2i(2 * tk));
+      const uint32_t mask = (1u << logcap) - 1u;
+      __syncthreads();
+      for (int i = tid; i < (1 << logcap); i += nthr) tab[i] = -1;
+      __syncthreads();
+      for (int i = tid; i < tk; i += nthr) {
+        int32_t key = radj[s0 + t0 + i];
+        uint32_t h = ((uint32_t)key * 2654435769u) >> (32 - logcap);
+        while (atomicCAS(&tab[h], -1, key) != -1) h = (h + 1) & mask;
+      }
+      __syncthreads();
+      HashTable t{tab, logcap};
+      c += scan_partners(roff, radj, padj, p0, p1, nl, t, wid, nw, lane);
+    }
+  }
+  __syncthreads();
+  return c;
+}
+
+__device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restrict__ roff,
+                                             const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
+                                             const int32_t *__restrict__ padj, const int32_t *__restrict__ plong,
+                                             uint32_t *words) {
+  const unsigned lane = lane_id();
+  const int64_t s0 = roff[x];
+  const int d = (int)(roff[x + 1] - s0);
+  const int64_t p0 = poff[x], p1 = poff[x + 1];
+  const int nl = plong[x];
+  const int32_t kmin = radj[s0], kmax = radj[s0 + d - 1];
+  const int64_t span = (int64_t)kmax - kmin + 1;
+  unsigned long long c = 0;
+  if (span <= (int64_t)kWarpWords * 32) {
+    const int nwords = (int)((span + 31) >> 5);
+    for (int i = lane; i < nwords; i += 32) words[i] = 0u;
+    __syncwarp();
+    for (int i = lane; i < d; i += 32) {
+      uint32_t o = (uint32_t)(radj[s0 + i] - kmin);
+      atomicOr(&words[o >> 5], 1u << (o & 31));
+    }
+    __syncwarp();
+    BitTable t{words, kmin, (uint32_t)span};
+    c = scan_partners(roff, radj, padj, p0, p1, nl, t, 0, 1, lane);
+  } else {
+    int32_t *tab = reinterpret_cast<int32_t *>(words);
+    for (int t0 = 0; t0 < d; t0 += kWarpHashChunk) {
+      const int tk = min(kWarpHashChunk, d - t0);
+      const int logcap = max(5, ceil_log2i(2 * tk));
+      const uint32_t mask = (1u << logcap) - 1u;
+      __syncwarp();
+      for (int i = lane; i < (1 << logcap); i += 32) tab[i] = -1;
+      __syncwarp();
+      for (int i = lane; i < tk; i += 32) {
+        int32_t key = radj[s0 + t0 + i];
+        uint32_t h = ((uint32_t)key * 2654435769u) >> (32 - logcap);
+        while (atomicCAS(&tab[h], -1, key) != -1) h = (h + 1) & mask;
+      }
+      __syncwarp();
+      HashTable t{tab, logcap};
+      c += scan_partners(roff, radj, padj, p0, p1, nl, t, 0, 1, lane);
+    }
+  }
+  __syncwarp();
+  return c;
+}
+
+__global__ void __launch_bounds__(256) k_tc_rank(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+                                                 const int64_t *__restrict__ poff, const int32_t *__restrict__ padj,
+                                                 const int32_t *__restrict__ plong,
+                                                 const int32_t *__restrict__ cta_tasks, int n_cta,
+                                                 const int32_t *__restrict__ warp_tasks, int n_warp,
+                                                 int *__restrict__ counters, unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) uint32_t rsm[];
+  __shared__ int s_task;
+  unsigned long long c = 0;
+  while (true) {
+    if (threadIdx.x == 0) s_task = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    int t = s_task;
+    __syncthreads();
+    if (t >= n_cta) break;
+    c += rank_cta_task(cta_tasks[t], roff, radj, poff, padj, plong, rsm);
+  }
+  const int wid = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t *region = rsm + wid * kWarpWords;
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&counters[1], 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= n_warp) break;
+    c += rank_warp_task(warp_tasks[t], roff, radj, poff, padj, plong, region);
+  }
+  c = warp_sum(c);
+  if (lane == 0 && c) atomicAdd(out, c);
+}
+
+// ------------------------------------------------------------ plan build
+__global__ void k_indeg(int64_t nnz, const int32_t *__restrict__ adj, int32_t *__restrict__ indeg) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&indeg[adj[i]], 1);
+}
+__global__ void k_rank_keys(int64_t n, const int64_t *__restrict__ off, const int32_t *__restrict__ indeg,
+                            uint32_t *__restrict__ key, int32_t *__restrict__ val) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    key[i] = (uint32_t)(off[i + 1] - off[i]) + (uint32_t)indeg[i];
+    val[i] = (int32_t)i;
+  }
+}
+__global__ void k_rank_inverse(int64_t n, const int32_t *__restrict__ order, const int64_t *__restrict__ off,
+                               int32_t *__restrict__ rank, int64_t *__restrict__ rdeg) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    int32_t v = order[r];
+    rank[v] = (int32_t)r;
+    rdeg[r] = off[v + 1] - off[v];
+  }
+}
+__global__ void k_rank_copy(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ rank,
+                            const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                            const int64_t *__restrict__ roff, int32_t *__restrict__ out) {
+  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < n; r += nw) {
+    int32_t v = order[r];
+    int64_t s = off[v], e = off[v + 1], o = roff[r];
+    for (int64_t k = s + lane_id(); k < e; k += 32) out[o + (k - s)] = rank[adj[k]];
+  }
+}
+
+// owner/partner assignment of every stored edge; long = partner list length >= long_min
+__global__ void k_partner_count(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+                                int long_min, int32_t *__restrict__ nlong, int32_t *__restrict__ nshort) {
+  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t u = warp; u < n; u += nw) {
+    int64_t s = roff[u], e = roff[u + 1], du = e - s;
+    for (int64_t k = s + lane_id(); k < e; k += 32) {
+      int32_t v = radj[k];
+      int64_t dv = roff[v + 1] - roff[v];
+      bool own_u = dv <= du;
+      int32_t owner = own_u ? (int32_t)u : v;
+      int64_t dp = own_u ? dv : du, dow = own_u ? du : dv;
+      if (dow < 2) continue;
+      atomicAdd(dp >= long_min ? &nlong[owner] : &nshort[owner], 1);
+    }
+  }
+}
+__global__ void k_partner_sizes(int64_t n, const int32_t *__restrict__ nlong, const int32_t *__restrict__ nshort,
+                                int64_t *__restrict__ tot) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    tot[i] = (int64_t)nlong[i] + nshort[i];
+}
+__global__ void k_partner_cursors(int64_t n, const int64_t *__restrict__ poff, const int32_t *__restrict__ nlong,
+                                  unsigned long long *__restrict__ curl, unsigned long long *__restrict__ curs) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    curl[i] = (unsigned long long)poff[i];
+    curs[i] = (unsigned long long)(poff[i] + nlong[i]);
+  }
+}
+__global__ void k_partner_fill(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+                               int long_min, unsigned long long *__restrict__ curl,
+                               unsigned long long *__restrict__ curs, int32_t *__restrict__ padj,
+                               unsigned long long *__restrict__ work) {
+  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t u = warp; u < n; u += nw) {
+    int64_t s = roff[u], e = roff[u + 1], du = e - s;
+    for (int64_t k = s + lane_id(); k < e; k += 32) {
+      int32_t v = radj[k];
+      int64_t dv = roff[v + 1] - roff[v];
+      bool own_u = dv <= du;
+      int32_t owner = own_u ? (int32_t)u : v, partner = own_u ? v : (int32_t)u;
+      int64_t dp = own_u ? dv : du, dow = own_u ? du : dv;
+      if (dow < 2) continue;
+      unsigned long long pos = atomicAdd(dp >= long_min ? &curl[owner] : &curs[owner], 1ull);
+      padj[pos] = partner;
+      atomicAdd(&work[owner], (unsigned long long)dp + 1ull);
+    }
+  }
+}
+// tasks: owners with partners; key = ~work so an ascending sort puts heavy first
+__global__ void k_rank_tasks(int64_t n, const int64_t *__restrict__ roff, const int64_t *__restrict__ poff,
+                             const unsigned long long *__restrict__ work, int cta_min,
+                             unsigned long long *__restrict__ ckey, int32_t *__restrict__ cval,
+                             unsigned long long *__restrict__ wkey, int32_t *__restrict__ wval,
+                             int *__restrict__ sizes) {
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+    if (poff[x + 1] == poff[x]) continue;
+    int64_t d = roff[x + 1] - roff[x];
+    if (d > cta_min) {
+      int i = atomicAdd(&sizes[0], 1);
+      ckey[i] = ~work[x];
+      cval[i] = (int32_t)x;
+    } else {
+      int i = atomicAdd(&sizes[1], 1);
+      wkey[i] = ~work[x];
+      wval[i] = (int32_t)x;
+    }
+  }
+}
+
+void free_rank_plan(RankPlan *p) { delete p; }
+
+static int sort_pairs_u64(DevBuf<unsigned long long> &k, DevBuf<int32_t> &v, int count, DevBuf<int32_t> &out,
+                          cudaStream_t st) {
+  if (count <= 0) return GPM_OK;
+  DevBuf<unsigned long long> k2;
+  GPM_TRY(k2.reserve(count));
+  size_t tmp = 0;
+  GPM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k.p, k2.p, v.p, out.p, count, 0, 64, st));
+  DevBuf<char> t;
+  GPM_TRY(t.reserve(tmp));
+  GPM_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, k.p, k2.p, v.p, out.p, count, 0, 64, st));
+  return GPM_OK;
+}
+
+static int scan_i64(int64_t n, const int64_t *cnt, int64_t *off, cudaStream_t st) {
+  size_t tmp = 0;
+  GPM_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, cnt, off + 1, (int)n, st));
+  DevBuf<char> t;
+  GPM_TRY(t.reserve(tmp));
+  GPM_CUDA(cudaMemsetAsync(off, 0, sizeof(int64_t), st));
+  if (n > 0) GPM_CUDA(cub::DeviceScan::InclusiveSum(t.p, tmp, cnt, off + 1, (int)n, st));
+  return GPM_OK;
+}
+
+int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
+  if (g->rank && g->rank->cta_min == cta_min && g->rank->long_min == long_min) return GPM_OK;
+  free_rank_plan(g->rank);
+  g->rank = nullptr;
+  const int64_t n = g->n, nnz = g->nnz;
+  RankPlan *p = new RankPlan();
+  p->cta_min = cta_min;
+  p->long_min = long_min;
+  auto bail = [&](int s) {
+    delete p;
+    return s;
+  };
+  int s;
+  // 1. rank by (in + out degree, id)
+  DevBuf<int32_t> indeg, val, order, rank;
+  DevBuf<uint32_t> key, key2;
+  DevBuf<int64_t> rdeg;
+  if ((s = indeg.reserve(n)) || (s = val.reserve(n)) || (s = order.reserve(n)) || (s = rank.reserve(n)) ||
+      (s = key.reserve(n)) || (s = key2.reserve(n)) || (s = rdeg.reserve(n)) || (s = p->roff.reserve(n + 1)) ||
+      (s = p->radj.reserve(nnz)) || (s = p->poff.reserve(n + 1)) || (s = p->padj.reserve(nnz)) ||
+      (s = p->plong.reserve(n)) || (s = p->counters.reserve(4)))
+    return bail(s);
+  cudaMemsetAsync(indeg.p, 0, sizeof(int32_t) * n, st);
+  k_indeg<<<grid_for(nnz), 256, 0, st>>>(nnz, g->adj.p, indeg.p);
+  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, indeg.p, key.p, val.p);
+  {
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, val.p, order.p, (int)n, 0, 32, st);
+    DevBuf<char> t;
+    if ((s = t.reserve(tmp))) return bail(s);
+    cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key2.p, val.p, order.p, (int)n, 0, 32, st);
+  }
+  k_rank_inverse<<<grid_for(n), 256, 0, st>>>(n, order.p, g->off.p, rank.p, rdeg.p);
+  if ((s = scan_i64(n, rdeg.p, p->roff.p, st))) return bail(s);
+  {
+    DevBuf<int32_t> tmpadj;
+    if ((s = tmpadj.reserve(nnz))) return bail(s);
+    k_rank_copy<<<grid_for(n * 32), 256, 0, st>>>(n, order.p, rank.p, g->off.p, g->adj.p, p->roff.p, tmpadj.p);
+    size_t tmp = 0;
+    cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, tmpadj.p, p->radj.p, (int)nnz, (int)n, p->roff.p,
+                                       p->roff.p + 1, st);
+    DevBuf<char> t;
+    if ((s = t.reserve(tmp))) return bail(s);
+    cub::DeviceSegmentedSort::SortKeys(t.p, tmp, tmpadj.p, p->radj.p, (int)nnz, (int)n, p->roff.p,
+                                       p->roff.p + 1, st);
+  }
+  // 2. owner / partner CSR
+  DevBuf<int32_t> nshort;
+  DevBuf<int64_t> tot;
+  DevBuf<unsigned long long> curl, curs, work;
+  if ((s = nshort.reserve(n)) || (s = tot.reserve(n)) || (s = curl.reserve(n)) || (s = curs.reserve(n)) ||
+      (s = work.reserve(n)))
+    return bail(s);
+  cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
+  cudaMemsetAsync(nshort.p, 0, sizeof(int32_t) * n, st);
+  cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
+  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, p->roff.p, p->radj.p, long_min, p->plong.p, nshort.p);
+  k_partner_sizes<<<grid_for(n), 256, 0, st>>>(n, p->plong.p, nshort.p, tot.p);
+  if ((s = scan_i64(n, tot.p, p->poff.p, st))) return bail(s);
+  k_partner_cursors<<<grid_for(n), 256, 0, st>>>(n, p->poff.p, p->plong.p, curl.p, curs.p);
+  k_partner_fill<<<grid_for(n * 32), 256, 0, st>>>(n, p->roff.p, p->radj.p, long_min, curl.p, curs.p, p->padj.p,
+                                                    work.p);
+  // 3. task queues, heaviest first
+  DevBuf<unsigned long long> ckey, wkey;
+  DevBuf<int32_t> cval, wval;
+  DevBuf<int> sizes;
+  if ((s = ckey.reserve(n)) || (s = wkey.reserve(n)) || (s = cval.reserve(n)) || (s = wval.reserve(n)) ||
+      (s = sizes.reserve(2)) || (s = p->cta_tasks.reserve(n)) || (s = p->warp_tasks.reserve(n)))
+    return bail(s);
+  cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st);
+  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, p->roff.p, p->poff.p, work.p, cta_min, ckey.p, cval.p, wkey.p,
+                                            wval.p, sizes.p);
+  int h[2] = {0, 0};
+  cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank plan: ") + cudaGetErrorString(e)));
+  p->n_cta = h[0];
+  p->n_warp = h[1];
+  if ((s = sort_pairs_u64(ckey, cval, h[0], p->cta_tasks, st)) || (s = sort_pairs_u64(wkey, wval, h[1], p->warp_tasks, st)))
+    return bail(s);
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank plan: ") + cudaGetErrorString(e)));
+  g->rank = p;
+  return GPM_OK;
+}
+
+static int rank_grid() {
+  static int grid = 0;
+  if (!grid) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_rank, 256, kRankSmem);
+    grid = std::max(1, per_sm) * num_sms();
+  }
+  return grid;
+}
+
+int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
+  GPM_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
+  if (g->nnz == 0) return GPM_OK;
+  // reference-style fixed thresholds: owners with > 100 keys go to a CTA
+  GPM_TRY(rank_build_plan(g, 100, 32, st));
+  RankPlan *p = g->rank;
+  GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 4 * sizeof(int), st));
+  k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(p->roff.p, p->radj.p, p->poff.p, p->padj.p, p->plong.p,
+                                                 p->cta_tasks.p, p->n_cta, p->warp_tasks.p, p->n_warp,
+                                                 p->counters.p, d_out);
+  GPM_LAUNCH_CHECK();
+  return GPM_OK;
+}
+
+}  // namespace gpm

@@ -19,7 +19,7 @@ GPM_OK = 0
 STATUS = {0: "GPM_OK", 1: "GPM_EINVAL", 2: "GPM_ECUDA", 3: "GPM_ENOMEM", 4: "GPM_EUNSUPPORTED",
           5: "GPM_ETIMEOUT", 6: "GPM_EIO", 7: "GPM_ENODEV"}
 V_CENTRIC, E_CENTRIC = 0, 1
-TC_AUTO, TC_BSEARCH, TC_HASH, TC_MERGE, TC_LEARNED = 0, 1, 2, 3, 4
+TC_AUTO, TC_BSEARCH, TC_HASH, TC_MERGE, TC_LEARNED, TC_BITMAP = 0, 1, 2, 3, 4, 5
 G2MINER, PATTERN_SOLVER = 0, 1
 SYMMETRIZE = 1
 
@@ -196,9 +196,9 @@ class Graph:
         return cls.generate(0, scale, edge_factor, a, b, c, seed)
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None) and lib is not None:
             lib.gpm_graph_destroy(self.h)
-            self.h = None
+        self.h = None
 
     __del__ = close
 
@@ -265,9 +265,9 @@ class Query:
         self.h = h
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None) and lib is not None:
             lib.gpm_query_destroy(self.h)
-            self.h = None
+        self.h = None
 
     __del__ = close
 

@@ -43,12 +43,14 @@ enum { GPM_V_CENTRIC = 0, GPM_E_CENTRIC = 1 };
 
 /* Triangle-count kernel variants (all return the same count). */
 enum {
-  GPM_TC_AUTO = 0,     /* engine's choice: learned scheduler if trained, else heuristic */
+  GPM_TC_AUTO = 0,     /* engine's default: GPM_TC_BITMAP                              */
   GPM_TC_BSEARCH = 1,  /* warp per stored edge, binary search (TCSolver.cuh:27-59 shape) */
   GPM_TC_HASH = 2,     /* vertex tasks, shared-memory hash of N(u), hub/tail queues
                           with the fixed thresholds of tuning_schedules.cuh:196-197   */
   GPM_TC_MERGE = 3,    /* warp per stored edge, merge-path intersection             */
-  GPM_TC_LEARNED = 4   /* per-task variant and split chosen by the MLP cost model   */
+  GPM_TC_LEARNED = 4,  /* per-task variant and split chosen by the MLP cost model   */
+  GPM_TC_BITMAP = 5    /* rank relabel, each edge from its shorter list, shared-memory
+                          bitmap membership (the engine's default)                 */
 };
 
 /* Pattern families: G2MinerSolver (src/G2MinerSolver.cuh) and PatternSolver

@@ -6,7 +6,7 @@ import gpm
 import _oracle as orc
 
 pytestmark = pytest.mark.gpu
-VARIANTS = [gpm.TC_BSEARCH, gpm.TC_MERGE, gpm.TC_HASH]
+VARIANTS = [gpm.TC_BSEARCH, gpm.TC_MERGE, gpm.TC_HASH, gpm.TC_BITMAP]
 
 
 def tc_all_variants(g):
