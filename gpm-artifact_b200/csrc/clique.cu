@@ -1,0 +1,455 @@
+// clique.cu -- k-clique counting (CFSolver, src/CFSolver.cuh:15-158).
+//
+// The reference counts, for every stored edge (v0,v1), the cliques grown by
+// nested materialised intersections W1 = N(v0) & N(v1), W2 = W1 & N(v2), ...
+// (clique_4_edge_warp / clique_5_edge_warp).  On a degree-oriented DAG that
+// is the number of k-cliques.
+//
+// B200 path (upward rank graph, see tc_rank.cuh): a vertex task u turns its
+// out-list L = N+(u) into a local DAG whose adjacency rows are bitsets
+// (row_i = {j : L[j] in N+(L[i])}).  Because the rank graph points upward,
+// row_i only has bits j > i, so the (k-1)-cliques of the local DAG are found
+// by consuming bits in increasing order and AND-ing rows -- popcounts instead
+// of list intersections.
+//   * tasks with |L| <= 64: one warp, rows are uint64 held in shared memory,
+//     one lane per starting row;
+//   * tasks with 64 < |L| <= 2048: one CTA, rows of W = ceil(|L|/32) words
+//     in shared memory (or a per-CTA global slab when they do not fit), each
+//     warp walks rows with the bitset spread over its lanes.
+// Graphs whose stored edges do not all point upward in rank order, or with
+// an out-list longer than 2048, use an edge-centric kernel shaped like the
+// reference (materialised lists in per-warp global scratch).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "motif.cuh"
+#include "tc_rank.cuh"
+
+namespace gpm {
+
+constexpr int kCqWarpMax = 64;      // warp tasks: |L| <= 64
+constexpr int kCqCtaMax = 2048;     // CTA tasks: |L| <= 2048 (W <= 64)
+constexpr int kCqMaxK = 8;
+constexpr size_t kCqSmem = 96 * 1024;  // dynamic shared memory per CTA
+
+static int grid_for(int64_t work, int block = 256) {
+  int64_t g = (work + block - 1) / block;
+  int64_t cap = (int64_t)num_sms() * 16;
+  return (int)std::max<int64_t>(1, std::min(g, cap));
+}
+
+// position of key in sorted L[0..d), or -1
+__device__ __forceinline__ int find_pos(const int32_t *L, int d, int32_t key) {
+  int lo = 0, hi = d - 1;
+  while (lo <= hi) {
+    int mid = (lo + hi) >> 1;
+    int32_t x = L[mid];
+    if (x == key) return mid;
+    if (x < key) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+// first index in sorted a[0..n) with a[i] > key
+__device__ __forceinline__ int64_t upper_bound_g(const int32_t *__restrict__ a, int64_t n, int32_t key) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (__ldg(a + mid) <= key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------------ warp tasks (|L| <= 64)
+// number of q-cliques inside bitset X of the local DAG (q >= 1)
+__device__ unsigned long long local_count64(const unsigned long long *rows, unsigned long long X, int q) {
+  if (q == 1) return __popcll(X);
+  if (q == 2) {
+    unsigned long long c = 0;
+    while (X) {
+      int l = __ffsll(X) - 1;
+      X &= X - 1;
+      c += __popcll(X & rows[l]);
+    }
+    return c;
+  }
+  unsigned long long stk[kCqMaxK];
+  int depth = 0;
+  stk[0] = X;
+  unsigned long long c = 0;
+  // stk[depth] holds the candidates still to extend at level depth; a set
+  // at level depth needs q - depth more vertices.
+  while (depth >= 0) {
+    unsigned long long &S = stk[depth];
+    if (!S) { --depth; continue; }
+    int l = __ffsll(S) - 1;
+    S &= S - 1;
+    unsigned long long Y = S & rows[l];
+    int left = q - depth - 1;  // vertices still needed after picking l
+    if (left == 1) c += __popcll(Y);
+    else if (left == 2) {
+      while (Y) {
+        int m = __ffsll(Y) - 1;
+        Y &= Y - 1;
+        c += __popcll(Y & rows[m]);
+      }
+    } else if (Y) stk[++depth] = Y;
+  }
+  return c;
+}
+
+__device__ unsigned long long clique_warp_task(int32_t u, int k, const int64_t *__restrict__ roff,
+                                               const int32_t *__restrict__ radj, int32_t *L,
+                                               unsigned long long *rows) {
+  const unsigned lane = lane_id();
+  const int64_t s0 = roff[u];
+  const int d = (int)(roff[u + 1] - s0);
+  for (int i = lane; i < d; i += 32) {
+    L[i] = radj[s0 + i];
+    rows[i] = 0ull;
+  }
+  __syncwarp();
+  const int32_t kmax = L[d - 1];
+  // row i: members of L inside N+(L[i]) (all > L[i]); scan up to kmax only
+  for (int i = 0; i < d; ++i) {
+    int32_t v = L[i];
+    int64_t s = roff[v], e = roff[v + 1];
+    int64_t stop = s;
+    if (lane == 0) stop = s + upper_bound_g(radj + s, e - s, kmax);
+    stop = __shfl_sync(0xffffffffu, stop, 0);
+    for (int64_t t = s + lane; t < stop; t += 32) {
+      int p = find_pos(L, d, __ldg(radj + t));
+      if (p >= 0) atomicOr(&rows[i], 1ull << p);
+    }
+  }
+  __syncwarp();
+  unsigned long long c = 0;
+  for (int i = lane; i < d; i += 32) c += local_count64(rows, rows[i], k - 2);
+  __syncwarp();
+  return c;
+}
+
+// ------------------------------------------------------------ CTA tasks (64 < |L| <= 2048)
+// Bitsets of W <= 64 words spread over a warp: lane w holds words w, w + 32.
+struct WarpSet {
+  uint32_t a, b;
+};
+__device__ __forceinline__ int wpop(WarpSet s) { return __popc(s.a) + __popc(s.b); }
+
+// Lowest set bit of a warp-spread set, cleared in place; -1 if empty.
+__device__ __forceinline__ int wtake(WarpSet &s, unsigned lane) {
+  unsigned m = __ballot_sync(0xffffffffu, s.a != 0);
+  int base = 0;
+  uint32_t word;
+  int f;
+  if (m) {
+    f = __ffs(m) - 1;
+    word = __shfl_sync(0xffffffffu, s.a, f);
+  } else {
+    m = __ballot_sync(0xffffffffu, s.b != 0);
+    if (!m) return -1;
+    f = __ffs(m) - 1;
+    word = __shfl_sync(0xffffffffu, s.b, f);
+    base = 1024;
+  }
+  int bit = __ffs(word) - 1;
+  if ((int)lane == f) {
+    if (base) s.b &= s.b - 1; else s.a &= s.a - 1;
+  }
+  return base + f * 32 + bit;
+}
+
+__device__ __forceinline__ WarpSet wrow(const uint32_t *rows, int W, int j, unsigned lane) {
+  const uint32_t *r = rows + (size_t)j * W;
+  WarpSet s;
+  s.a = (int)lane < W ? r[lane] : 0u;
+  s.b = (int)lane + 32 < W ? r[lane + 32] : 0u;
+  return s;
+}
+
+// q-cliques inside warp-spread X; stk holds (q) levels of W words per warp
+__device__ unsigned long long warp_count_set(const uint32_t *rows, int W, WarpSet X, int q, unsigned lane) {
+  if (q == 1) return (unsigned long long)wpop(X);
+  WarpSet stk[kCqMaxK];
+  int depth = 0;
+  stk[0] = X;
+  unsigned long long c = 0;
+  while (depth >= 0) {
+    int l = wtake(stk[depth], lane);
+    if (l < 0) { --depth; continue; }
+    WarpSet r = wrow(rows, W, l, lane);
+    WarpSet Y{stk[depth].a & r.a, stk[depth].b & r.b};
+    int left = q - depth - 1;
+    if (left == 1) c += (unsigned long long)wpop(Y);
+    else stk[++depth] = Y;
+  }
+  return c;
+}
+
+__device__ unsigned long long clique_cta_task(int32_t u, int k, const int64_t *__restrict__ roff,
+                                              const int32_t *__restrict__ radj, char *smem, uint32_t *slab) {
+  const int tid = threadIdx.x, nthr = blockDim.x, wid = tid >> 5, nw = nthr >> 5;
+  const unsigned lane = tid & 31;
+  const int64_t s0 = roff[u];
+  const int d = (int)(roff[u + 1] - s0);
+  const int W = (d + 31) >> 5;
+  int32_t *L = reinterpret_cast<int32_t *>(smem);
+  size_t lbytes = ((size_t)d * 4 + 15) & ~(size_t)15;
+  size_t rbytes = (size_t)d * W * 4;
+  uint32_t *rows = lbytes + rbytes <= kCqSmem ? reinterpret_cast<uint32_t *>(smem + lbytes) : slab;
+  for (int i = tid; i < d; i += nthr) L[i] = radj[s0 + i];
+  for (size_t i = tid; i < (size_t)d * W; i += nthr) rows[i] = 0u;
+  __syncthreads();
+  const int32_t kmax = L[d - 1];
+  for (int i = wid; i < d; i += nw) {
+    int32_t v = L[i];
+    int64_t s = roff[v], e = roff[v + 1];
+    int64_t stop = s;
+    if (lane == 0) stop = s + upper_bound_g(radj + s, e - s, kmax);
+    stop = __shfl_sync(0xffffffffu, stop, 0);
+    uint32_t *ri = rows + (size_t)i * W;
+    for (int64_t t = s + lane; t < stop; t += 32) {
+      int p = find_pos(L, d, __ldg(radj + t));
+      if (p >= 0) atomicOr(&ri[p >> 5], 1u << (p & 31));
+    }
+  }
+  __syncthreads();
+  unsigned long long c = 0;
+  // each lane accumulates the popcounts of its own words; the warp sum is the count
+  for (int i = wid; i < d; i += nw) c += warp_count_set(rows, W, wrow(rows, W, i, lane), k - 2, lane);
+  __syncthreads();
+  return c;
+}
+
+__global__ void __launch_bounds__(256) k_clique_local(int k, const int64_t *__restrict__ roff,
+                                                      const int32_t *__restrict__ radj,
+                                                      const int32_t *__restrict__ cta_tasks, int n_cta,
+                                                      const int32_t *__restrict__ warp_tasks, int n_warp,
+                                                      int *__restrict__ counters, uint32_t *__restrict__ slabs,
+                                                      size_t slab_words, const int32_t *__restrict__ gid,
+                                                      unsigned long long *__restrict__ acc, int stride, int slot) {
+  extern __shared__ __align__(16) char csm[];
+  __shared__ int s_task;
+  const int wid = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t *slab = slabs + (size_t)blockIdx.x * slab_words;
+  while (true) {
+    if (threadIdx.x == 0) s_task = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    int t = s_task;
+    __syncthreads();
+    if (t >= n_cta) break;
+    const int32_t u = cta_tasks[t];
+    unsigned long long c = warp_sum(clique_cta_task(u, k, roff, radj, csm, slab));
+    if (lane == 0 && c) atomicAdd(&acc[(size_t)stride * (gid ? gid[u] : 0) + slot], c);
+  }
+  int32_t *L = reinterpret_cast<int32_t *>(csm + wid * (kCqWarpMax * 12));
+  unsigned long long *rows = reinterpret_cast<unsigned long long *>(csm + wid * (kCqWarpMax * 12) + kCqWarpMax * 4);
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&counters[1], 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= n_warp) break;
+    const int32_t u = warp_tasks[t];
+    unsigned long long c = warp_sum(clique_warp_task(u, k, roff, radj, L, rows));
+    if (lane == 0 && c) atomicAdd(&acc[(size_t)stride * (gid ? gid[u] : 0) + slot], c);
+  }
+}
+
+__global__ void k_clique_tasks(int64_t n, const int64_t *__restrict__ roff, int k, uint32_t *__restrict__ ckey,
+                               int32_t *__restrict__ cval, uint32_t *__restrict__ wkey, int32_t *__restrict__ wval,
+                               int *__restrict__ sizes) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+    int64_t d = roff[u + 1] - roff[u];
+    if (d < k - 1) continue;
+    if (d > kCqWarpMax) {
+      int i = atomicAdd(&sizes[0], 1);
+      ckey[i] = ~(uint32_t)d;
+      cval[i] = (int32_t)u;
+    } else {
+      int i = atomicAdd(&sizes[1], 1);
+      wkey[i] = ~(uint32_t)d;
+      wval[i] = (int32_t)u;
+    }
+  }
+}
+
+// ------------------------------------------------------------ edge-centric (reference-shaped)
+// Warp-cooperative c = a & b by binary search of the shorter list's keys in
+// the longer one, compacted in order with ballots; returns |c|.
+__device__ int warp_isect_store(const int32_t *a, int na, const int32_t *b, int nb, int32_t *c, unsigned lane) {
+  const int32_t *look = a, *srch = b;
+  int nl = na, ns = nb;
+  if (na > nb) { look = b; srch = a; nl = nb; ns = na; }
+  int cnt = 0;
+  for (int base = 0; base < nl; base += 32) {
+    int i = base + lane;
+    bool f = false;
+    int32_t key = 0;
+    if (i < nl) {
+      key = look[i];
+      int lo = 0, hi = ns - 1;
+      while (lo <= hi) {
+        int mid = (lo + hi) >> 1;
+        int32_t x = srch[mid];
+        if (x == key) { f = true; break; }
+        if (x < key) lo = mid + 1; else hi = mid - 1;
+      }
+    }
+    unsigned m = __ballot_sync(0xffffffffu, f);
+    if (f) c[cnt + __popc(m & ((1u << lane) - 1u))] = key;
+    cnt += __popc(m);
+  }
+  __syncwarp();
+  return cnt;
+}
+
+__device__ unsigned long long warp_isect_count(const int32_t *a, int na, const int32_t *b, int nb, unsigned lane) {
+  const int32_t *look = a, *srch = b;
+  int nl = na, ns = nb;
+  if (na > nb) { look = b; srch = a; nl = nb; ns = na; }
+  unsigned long long c = 0;
+  for (int i = lane; i < nl; i += 32) {
+    int32_t key = look[i];
+    int lo = 0, hi = ns - 1;
+    while (lo <= hi) {
+      int mid = (lo + hi) >> 1;
+      int32_t x = srch[mid];
+      if (x == key) { ++c; break; }
+      if (x < key) lo = mid + 1; else hi = mid - 1;
+    }
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(256) k_clique_edge(int64_t nnz, int k, const int64_t *__restrict__ off,
+                                                     const int32_t *__restrict__ adj, const int32_t *__restrict__ src,
+                                                     int32_t *__restrict__ scratch, int maxd,
+                                                     unsigned long long *__restrict__ out) {
+  const unsigned lane = lane_id();
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  int32_t *lists = scratch + warp * (int64_t)maxd * (kCqMaxK - 2);
+  int sizes[kCqMaxK], cursor[kCqMaxK];
+  unsigned long long c = 0;
+  for (int64_t e = warp; e < nnz; e += nw) {
+    int32_t v0 = src[e], v1 = adj[e];
+    int n1 = warp_isect_store(adj + off[v0], (int)(off[v0 + 1] - off[v0]), adj + off[v1],
+                              (int)(off[v1 + 1] - off[v1]), lists, lane);
+    // lists[l] holds the candidates after l+2 clique vertices
+    if (k == 3) { c += lane == 0 ? (unsigned long long)n1 : 0ull; continue; }
+    sizes[0] = n1;
+    cursor[0] = 0;
+    int depth = 0;
+    while (depth >= 0) {
+      if (cursor[depth] >= sizes[depth]) { --depth; continue; }
+      int32_t *cur = lists + (int64_t)depth * maxd;
+      int32_t x = cur[cursor[depth]++];
+      const int32_t *nx = adj + off[x];
+      int dx = (int)(off[x + 1] - off[x]);
+      if (depth + 3 == k - 1) {
+        c += warp_isect_count(cur, sizes[depth], nx, dx, lane);
+      } else {
+        int32_t *nxt = lists + (int64_t)(depth + 1) * maxd;
+        sizes[depth + 1] = warp_isect_store(cur, sizes[depth], nx, dx, nxt, lane);
+        cursor[depth + 1] = 0;
+        ++depth;
+      }
+    }
+  }
+  c = warp_sum(c);
+  if (lane == 0 && c) atomicAdd(out, c);
+}
+
+// ------------------------------------------------------------ host
+static int clique_local_grid() {
+  static int grid = 0;
+  if (!grid) {
+    cudaFuncSetAttribute(k_clique_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCqSmem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_local, 256, kCqSmem);
+    grid = std::max(1, per_sm) * num_sms();
+  }
+  return grid;
+}
+
+int clique_run_upward(int64_t n, const int64_t *roff, const int32_t *radj, int max_deg, int k, const int32_t *gid,
+                      unsigned long long *acc, int stride, int slot, cudaStream_t st) {
+  if (n == 0) return GPM_OK;
+  if (max_deg > kCqCtaMax) return fail(GPM_EUNSUPPORTED, "out-list longer than 2048 on the bitset clique path");
+  DevBuf<uint32_t> ckey, wkey;
+  DevBuf<int32_t> cval, wval, ctasks, wtasks;
+  DevBuf<int> sizes, counters;
+  GPM_TRY(ckey.reserve(n));
+  GPM_TRY(wkey.reserve(n));
+  GPM_TRY(cval.reserve(n));
+  GPM_TRY(wval.reserve(n));
+  GPM_TRY(ctasks.reserve(n));
+  GPM_TRY(wtasks.reserve(n));
+  GPM_TRY(sizes.reserve(2));
+  GPM_TRY(counters.reserve(2));
+  GPM_CUDA(cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st));
+  GPM_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(int), st));
+  k_clique_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, k, ckey.p, cval.p, wkey.p, wval.p, sizes.p);
+  int h[2];
+  GPM_CUDA(cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st));
+  GPM_CUDA(cudaStreamSynchronize(st));
+  for (int which = 0; which < 2; ++which) {
+    int cnt = h[which];
+    if (cnt <= 0) continue;
+    DevBuf<uint32_t> k2;
+    GPM_TRY(k2.reserve(cnt));
+    size_t tmp = 0;
+    uint32_t *kin = which ? wkey.p : ckey.p;
+    int32_t *vin = which ? wval.p : cval.p, *vout = which ? wtasks.p : ctasks.p;
+    GPM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kin, k2.p, vin, vout, cnt, 0, 32, st));
+    DevBuf<char> t;
+    GPM_TRY(t.reserve(tmp));
+    GPM_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kin, k2.p, vin, vout, cnt, 0, 32, st));
+  }
+  // per-CTA slabs for rows that do not fit in shared memory
+  int grid = clique_local_grid();
+  size_t W = (size_t)(max_deg + 31) / 32;
+  size_t slab_words = (size_t)max_deg * W * 4 + (size_t)max_deg * 4 > kCqSmem ? (size_t)max_deg * W : 1;
+  DevBuf<uint32_t> slabs;
+  GPM_TRY(slabs.reserve(slab_words * grid));
+  k_clique_local<<<grid, 256, kCqSmem, st>>>(k, roff, radj, ctasks.p, h[0], wtasks.p, h[1], counters.p, slabs.p,
+                                             slab_words, gid, acc, stride, slot);
+  GPM_LAUNCH_CHECK();
+  GPM_CUDA(cudaStreamSynchronize(st));  // the scratch above is released on return
+  return GPM_OK;
+}
+
+int clique_launch(gpm_graph *g, int k, cudaStream_t st, unsigned long long *d_out) {
+  GPM_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
+  if (g->nnz == 0) return GPM_OK;
+  GPM_TRY(ensure_rank_graph(g, st));
+  if (g->rg->upward && g->max_deg <= kCqCtaMax)
+    return clique_run_upward(g->n, g->rg->roff.p, g->rg->radj.p, g->max_deg, k, nullptr, d_out, 0, 0, st);
+  // edge-centric path on the stored graph
+  GPM_TRY(ensure_src(g, st));
+  int grid = num_sms() * 8;
+  int64_t warps = (int64_t)grid * 8;
+  int maxd = std::max(1, g->max_deg);
+  DevBuf<int32_t> scratch;
+  GPM_TRY(scratch.reserve((size_t)warps * maxd * (kCqMaxK - 2)));
+  k_clique_edge<<<grid, 256, 0, st>>>(g->nnz, k, g->off.p, g->adj.p, g->src.p, scratch.p, maxd, d_out);
+  GPM_LAUNCH_CHECK();
+  GPM_CUDA(cudaStreamSynchronize(st));
+  return GPM_OK;
+}
+
+}  // namespace gpm
+
+using namespace gpm;
+
+extern "C" int gpm_clique(gpm_graph *g, int k, uint64_t *out) {
+  if (!g || !out) return fail(GPM_EINVAL, "gpm_clique: NULL argument");
+  if (k < 3 || k > kCqMaxK) return fail(GPM_EUNSUPPORTED, "k-clique supports 3 <= k <= 8");
+  GPM_TRY(g->result.reserve(8));
+  GPM_TRY(clique_launch(g, k, 0, (unsigned long long *)g->result.p));
+  GPM_CUDA(cudaMemcpy(out, g->result.p, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return GPM_OK;
+}

@@ -150,6 +150,7 @@ __device__ __forceinline__ T warp_sum(T v) {
 // ---------------------------------------------------------------- graph handle
 struct TcPlan;
 struct RankPlan;
+struct RankGraph;
 struct MotifPlan;
 
 }  // namespace gpm
@@ -167,6 +168,7 @@ struct gpm_graph {
   gpm::DevBuf<int32_t> src;     // nnz, COO source of each stored entry (lazy)
   gpm::TcPlan *tc = nullptr;    // cached triangle-count schedule (HASH)
   gpm::RankPlan *rank = nullptr; // cached schedule of the BITMAP path
+  gpm::RankGraph *rg = nullptr;  // cached rank-relabelled copy
   gpm::DevBuf<uint64_t> result; // small device result scratch
   ~gpm_graph();
 };
@@ -179,5 +181,8 @@ int ensure_src(gpm_graph *g, cudaStream_t st);
 int compute_max_degree(gpm_graph *g, cudaStream_t st);
 void free_tc_plan(TcPlan *p);
 void free_rank_plan(RankPlan *p);
+void free_rank_graph(RankGraph *r);
+// Drops every cached schedule (after the stored graph changed).
+void drop_plans(gpm_graph *g);
 int num_sms();
 }  // namespace gpm

@@ -377,10 +377,18 @@ __global__ void k_work(int64_t n, const int64_t *__restrict__ off, const int32_t
 
 using namespace gpm;
 
-gpm_graph::~gpm_graph() {
-  free_tc_plan(tc);
-  free_rank_plan(rank);
+namespace gpm {
+void drop_plans(gpm_graph *g) {
+  free_tc_plan(g->tc);
+  g->tc = nullptr;
+  free_rank_plan(g->rank);
+  g->rank = nullptr;
+  free_rank_graph(g->rg);
+  g->rg = nullptr;
 }
+}  // namespace gpm
+
+gpm_graph::~gpm_graph() { drop_plans(this); }
 
 extern "C" {
 
@@ -544,10 +552,7 @@ int gpm_graph_set_labels(gpm_graph *g, const int32_t *labels) {
 
 int gpm_graph_orient(gpm_graph *g, int relabel) {
   if (!g) return fail(GPM_EINVAL, "NULL graph");
-  free_tc_plan(g->tc);
-  g->tc = nullptr;
-  free_rank_plan(g->rank);
-  g->rank = nullptr;
+  drop_plans(g);
   GPM_TRY(orient_on_stream(g, 0));
   if (relabel) GPM_TRY(relabel_device(g, 0));
   GPM_TRY(compute_max_degree(g, 0));

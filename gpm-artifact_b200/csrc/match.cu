@@ -1,0 +1,261 @@
+// match.cu -- labelled subgraph matching with sub_ceci's semantics.
+//
+// sub_ceci (sub_ceci/myceci.cpp:540-668) counts every injective map phi of
+// the query vertices into the data graph with label(phi(u)) == label(u) and
+// every query edge mapped onto a data edge (non-induced; automorphic images
+// are separate embeddings).  Its CECI filter and tree only prune; the count
+// is that number.
+//
+// GPU design: the query (<= 16 vertices) is ordered on the host -- start at
+// the vertex whose label is rarest in the data graph (ties: higher degree),
+// then repeatedly the unplaced vertex with most placed neighbours.  Each
+// later vertex has a parent (its first placed neighbour, whose data
+// neighbours are the candidates) and back-neighbours (checked by binary
+// search in their images' sorted lists).  One warp per root candidate runs
+// the depth-first extension: a level's candidates are filtered by label,
+// degree, injectivity and back-edges 32 at a time and compacted with ballots
+// into per-warp scratch; the last level is only counted.  Work is drained
+// from an atomic root cursor.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+constexpr int kMaxQ = 16;
+
+struct gpm_query {
+  int n = 0;
+  int32_t labels[kMaxQ];
+  uint32_t adjmask[kMaxQ];  // bit j set iff query edge (i, j)
+  int deg[kMaxQ];
+};
+
+namespace gpm {
+
+struct QueryPlan {
+  int n;
+  int order[kMaxQ];
+  int parent_pos[kMaxQ];      // position (in order) of the parent, -1 for the root
+  uint32_t back_pos[kMaxQ];   // bitmask of earlier positions that must be adjacent (parent excluded)
+  int32_t label[kMaxQ];       // label of the vertex at each position
+  int mindeg[kMaxQ];          // query degree at each position
+};
+
+__device__ __forceinline__ bool has_edge(const int64_t *__restrict__ off, const int32_t *__restrict__ adj, int32_t a,
+                                         int32_t key) {
+  int64_t lo = off[a], hi = off[a + 1] - 1;
+  while (lo <= hi) {
+    int64_t mid = (lo + hi) >> 1;
+    int32_t x = __ldg(adj + mid);
+    if (x == key) return true;
+    if (x < key) lo = mid + 1; else hi = mid - 1;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(256) k_match(QueryPlan q, int64_t n, const int64_t *__restrict__ off,
+                                               const int32_t *__restrict__ adj, const int32_t *__restrict__ labels,
+                                               int32_t *__restrict__ scratch, int64_t maxd, int *__restrict__ cursor,
+                                               unsigned long long *__restrict__ out) {
+  const unsigned lane = lane_id();
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  int32_t *lists = scratch + warp * maxd * (kMaxQ - 1);
+  int32_t emb[kMaxQ];
+  int cur[kMaxQ], sz[kMaxQ];
+  unsigned long long c = 0;
+  while (true) {
+    int64_t r = 0;
+    if (lane == 0) r = atomicAdd(cursor, 1);
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if (r >= n) break;
+    const int32_t v0 = (int32_t)r;
+    if (labels[v0] != q.label[0] || off[v0 + 1] - off[v0] < q.mindeg[0]) continue;
+    if (q.n == 1) {
+      c += lane == 0;
+      continue;
+    }
+    emb[0] = v0;
+    int depth = 1;  // position being filled
+    bool build = true;
+    while (depth >= 1) {
+      if (build) {
+        // candidates of position `depth`: neighbours of the parent's image
+        const int32_t pv = emb[q.parent_pos[depth]];
+        const int64_t s = off[pv], e = off[pv + 1];
+        const bool last = depth == q.n - 1;
+        int32_t *L = lists + (int64_t)(depth - 1) * maxd;
+        int cnt = 0;
+        for (int64_t base = s; base < e; base += 32) {
+          int64_t i = base + lane;
+          bool ok = false;
+          int32_t x = 0;
+          if (i < e) {
+            x = __ldg(adj + i);
+            ok = labels[x] == q.label[depth] && off[x + 1] - off[x] >= q.mindeg[depth];
+            for (int j = 0; ok && j < depth; ++j) ok = emb[j] != x;
+            uint32_t bm = q.back_pos[depth];
+            while (ok && bm) {
+              int j = __ffs(bm) - 1;
+              bm &= bm - 1;
+              ok = has_edge(off, adj, emb[j], x);
+            }
+          }
+          unsigned m = __ballot_sync(0xffffffffu, ok);
+          if (!last && ok) L[cnt + __popc(m & ((1u << lane) - 1u))] = x;
+          cnt += __popc(m);
+        }
+        __syncwarp();
+        if (last) {
+          c += lane == 0 ? (unsigned long long)cnt : 0ull;
+          --depth;
+          build = false;
+          continue;
+        }
+        sz[depth] = cnt;
+        cur[depth] = 0;
+        build = false;
+      }
+      if (cur[depth] >= sz[depth]) {
+        --depth;
+        continue;
+      }
+      emb[depth] = lists[(int64_t)(depth - 1) * maxd + cur[depth]++];
+      ++depth;
+      build = true;
+    }
+  }
+  c = warp_sum(c);
+  if (lane == 0 && c) atomicAdd(out, c);
+}
+
+static int plan_query(const gpm_query *q, const std::vector<int64_t> &label_freq, QueryPlan *p) {
+  const int n = q->n;
+  p->n = n;
+  bool placed[kMaxQ] = {false};
+  int best = 0;
+  auto freq = [&](int u) -> int64_t {
+    int32_t l = q->labels[u];
+    return (l >= 0 && (size_t)l < label_freq.size()) ? label_freq[l] : 0;
+  };
+  for (int u = 1; u < n; ++u)
+    if (freq(u) < freq(best) || (freq(u) == freq(best) && q->deg[u] > q->deg[best])) best = u;
+  p->order[0] = best;
+  placed[best] = true;
+  for (int k = 1; k < n; ++k) {
+    int b = -1, bs = -1, bd = -1;
+    for (int u = 0; u < n; ++u) {
+      if (placed[u]) continue;
+      int s = 0;
+      for (int w = 0; w < n; ++w) s += placed[w] && ((q->adjmask[u] >> w) & 1u);
+      if (s > bs || (s == bs && q->deg[u] > bd)) {
+        b = u;
+        bs = s;
+        bd = q->deg[u];
+      }
+    }
+    if (bs <= 0) return fail(GPM_EUNSUPPORTED, "query graph must be connected");
+    p->order[k] = b;
+    placed[b] = true;
+  }
+  for (int k = 0; k < n; ++k) {
+    int u = p->order[k];
+    p->label[k] = q->labels[u];
+    p->mindeg[k] = q->deg[u];
+    p->parent_pos[k] = -1;
+    p->back_pos[k] = 0;
+    for (int j = 0; j < k; ++j) {
+      if (!((q->adjmask[u] >> p->order[j]) & 1u)) continue;
+      if (p->parent_pos[k] < 0) p->parent_pos[k] = j;
+      else p->back_pos[k] |= 1u << j;
+    }
+  }
+  return GPM_OK;
+}
+
+__global__ void k_label_hist(int64_t n, const int32_t *__restrict__ labels, int nl, unsigned long long *__restrict__ h) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int32_t l = labels[i];
+    if (l >= 0 && l < nl) atomicAdd(&h[l], 1ull);
+  }
+}
+
+}  // namespace gpm
+
+using namespace gpm;
+
+extern "C" {
+
+int gpm_query_create(int64_t n, int64_t m, const int32_t *src, const int32_t *dst, const int32_t *labels,
+                     gpm_query **out) {
+  if (!out || !labels || n < 1 || m < 0 || (m > 0 && (!src || !dst)))
+    return fail(GPM_EINVAL, "gpm_query_create: bad argument");
+  if (n > kMaxQ) return fail(GPM_EUNSUPPORTED, "query graphs are limited to 16 vertices");
+  gpm_query *q = new gpm_query();
+  q->n = (int)n;
+  for (int i = 0; i < n; ++i) {
+    q->labels[i] = labels[i];
+    q->adjmask[i] = 0;
+  }
+  for (int64_t e = 0; e < m; ++e) {
+    int a = src[e], b = dst[e];
+    if (a < 0 || b < 0 || a >= n || b >= n) {
+      delete q;
+      return fail(GPM_EINVAL, "query edge out of range");
+    }
+    if (a == b) continue;
+    q->adjmask[a] |= 1u << b;
+    q->adjmask[b] |= 1u << a;
+  }
+  for (int i = 0; i < n; ++i) q->deg[i] = __builtin_popcount(q->adjmask[i]);
+  *out = q;
+  return GPM_OK;
+}
+
+int gpm_query_destroy(gpm_query *q) {
+  delete q;
+  return GPM_OK;
+}
+
+int gpm_match(gpm_graph *g, const gpm_query *q, uint64_t *out) {
+  if (!g || !q || !out) return fail(GPM_EINVAL, "gpm_match: NULL argument");
+  if (!g->labels.p) return fail(GPM_EINVAL, "the data graph carries no labels");
+  if (g->oriented) return fail(GPM_EINVAL, "matching needs the symmetric (unoriented) data graph");
+  // label frequencies pick the root
+  int maxl = 0;
+  for (int i = 0; i < q->n; ++i) maxl = std::max(maxl, q->labels[i] + 1);
+  std::vector<int64_t> freq(maxl, 0);
+  {
+    DevBuf<unsigned long long> h;
+    GPM_TRY(h.reserve(maxl));
+    GPM_CUDA(cudaMemset(h.p, 0, sizeof(unsigned long long) * maxl));
+    if (g->n > 0) k_label_hist<<<(int)std::min<int64_t>((g->n + 255) / 256, num_sms() * 8), 256>>>(g->n, g->labels.p, maxl, h.p);
+    std::vector<unsigned long long> hh(maxl);
+    GPM_CUDA(cudaMemcpy(hh.data(), h.p, sizeof(unsigned long long) * maxl, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < maxl; ++i) freq[i] = (int64_t)hh[i];
+  }
+  QueryPlan plan;
+  GPM_TRY(plan_query(q, freq, &plan));
+  const int64_t maxd = std::max(1, g->max_deg);
+  int64_t warps = (int64_t)num_sms() * 4 * 8;
+  const int64_t cap_words = (int64_t)2 << 30;
+  while (warps > 32 && warps * maxd * (kMaxQ - 1) > cap_words) warps >>= 1;
+  DevBuf<int32_t> scratch;
+  DevBuf<int> cursor;
+  DevBuf<unsigned long long> d;
+  GPM_TRY(scratch.reserve((size_t)(warps * maxd * (kMaxQ - 1))));
+  GPM_TRY(cursor.reserve(1));
+  GPM_TRY(d.reserve(1));
+  GPM_CUDA(cudaMemset(cursor.p, 0, sizeof(int)));
+  GPM_CUDA(cudaMemset(d.p, 0, 8));
+  if (g->n > 0) {
+    k_match<<<(int)(warps / 8), 256>>>(plan, g->n, g->off.p, g->adj.p, g->labels.p, scratch.p, maxd, cursor.p, d.p);
+    GPM_LAUNCH_CHECK();
+  }
+  unsigned long long h = 0;
+  GPM_CUDA(cudaMemcpy(&h, d.p, 8, cudaMemcpyDeviceToHost));
+  *out = h;
+  return GPM_OK;
+}
+
+}  // extern "C"

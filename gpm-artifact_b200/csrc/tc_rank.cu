@@ -370,10 +370,74 @@ static int scan_i64(int64_t n, const int64_t *cnt, int64_t *off, cudaStream_t st
   return GPM_OK;
 }
 
+__global__ void k_count_down(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+                             int *__restrict__ down) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x)
+    if (roff[u + 1] > roff[u] && radj[roff[u]] <= (int32_t)u) atomicAdd(down, 1);
+}
+
+void free_rank_graph(RankGraph *r) { delete r; }
+
+// Renumber the stored graph by (in + out degree, id) rank; lists re-sorted.
+int ensure_rank_graph(gpm_graph *g, cudaStream_t st) {
+  if (g->rg) return GPM_OK;
+  const int64_t n = g->n, nnz = g->nnz;
+  RankGraph *r = new RankGraph();
+  auto bail = [&](int s) {
+    delete r;
+    return s;
+  };
+  int s;
+  DevBuf<int32_t> indeg, val, rank;
+  DevBuf<uint32_t> key, key2;
+  DevBuf<int64_t> rdeg;
+  DevBuf<int> down;
+  if ((s = indeg.reserve(n)) || (s = val.reserve(n)) || (s = r->order.reserve(n)) || (s = rank.reserve(n)) ||
+      (s = key.reserve(n)) || (s = key2.reserve(n)) || (s = rdeg.reserve(n)) || (s = r->roff.reserve(n + 1)) ||
+      (s = r->radj.reserve(nnz)) || (s = down.reserve(1)))
+    return bail(s);
+  int32_t *order = r->order.p;
+  cudaMemsetAsync(indeg.p, 0, sizeof(int32_t) * n, st);
+  k_indeg<<<grid_for(nnz), 256, 0, st>>>(nnz, g->adj.p, indeg.p);
+  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, indeg.p, key.p, val.p);
+  {
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, val.p, order, (int)n, 0, 32, st);
+    DevBuf<char> t;
+    if ((s = t.reserve(tmp))) return bail(s);
+    cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key2.p, val.p, order, (int)n, 0, 32, st);
+  }
+  k_rank_inverse<<<grid_for(n), 256, 0, st>>>(n, order, g->off.p, rank.p, rdeg.p);
+  if ((s = scan_i64(n, rdeg.p, r->roff.p, st))) return bail(s);
+  {
+    DevBuf<int32_t> tmpadj;
+    if ((s = tmpadj.reserve(nnz))) return bail(s);
+    k_rank_copy<<<grid_for(n * 32), 256, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, r->roff.p, tmpadj.p);
+    size_t tmp = 0;
+    cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, tmpadj.p, r->radj.p, (int)nnz, (int)n, r->roff.p,
+                                       r->roff.p + 1, st);
+    DevBuf<char> t;
+    if ((s = t.reserve(tmp))) return bail(s);
+    cub::DeviceSegmentedSort::SortKeys(t.p, tmp, tmpadj.p, r->radj.p, (int)nnz, (int)n, r->roff.p,
+                                       r->roff.p + 1, st);
+  }
+  // does every stored edge point to a larger rank? (true for a degree-oriented DAG)
+  cudaMemsetAsync(down.p, 0, sizeof(int), st);
+  k_count_down<<<grid_for(n), 256, 0, st>>>(n, r->roff.p, r->radj.p, down.p);
+  int hdown = 0;
+  cudaMemcpyAsync(&hdown, down.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank relabel: ") + cudaGetErrorString(e)));
+  r->upward = hdown == 0;
+  g->rg = r;
+  return GPM_OK;
+}
+
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
   if (g->rank && g->rank->cta_min == cta_min && g->rank->long_min == long_min) return GPM_OK;
   free_rank_plan(g->rank);
   g->rank = nullptr;
+  GPM_TRY(ensure_rank_graph(g, st));
   const int64_t n = g->n, nnz = g->nnz;
   RankPlan *p = new RankPlan();
   p->cta_min = cta_min;
@@ -383,39 +447,11 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
     return s;
   };
   int s;
-  // 1. rank by (in + out degree, id)
-  DevBuf<int32_t> indeg, val, order, rank;
-  DevBuf<uint32_t> key, key2;
-  DevBuf<int64_t> rdeg;
-  if ((s = indeg.reserve(n)) || (s = val.reserve(n)) || (s = order.reserve(n)) || (s = rank.reserve(n)) ||
-      (s = key.reserve(n)) || (s = key2.reserve(n)) || (s = rdeg.reserve(n)) || (s = p->roff.reserve(n + 1)) ||
-      (s = p->radj.reserve(nnz)) || (s = p->poff.reserve(n + 1)) || (s = p->padj.reserve(nnz)) ||
-      (s = p->plong.reserve(n)) || (s = p->counters.reserve(4)))
+  if ((s = p->poff.reserve(n + 1)) || (s = p->padj.reserve(nnz)) || (s = p->plong.reserve(n)) ||
+      (s = p->counters.reserve(4)))
     return bail(s);
-  cudaMemsetAsync(indeg.p, 0, sizeof(int32_t) * n, st);
-  k_indeg<<<grid_for(nnz), 256, 0, st>>>(nnz, g->adj.p, indeg.p);
-  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, indeg.p, key.p, val.p);
-  {
-    size_t tmp = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, val.p, order.p, (int)n, 0, 32, st);
-    DevBuf<char> t;
-    if ((s = t.reserve(tmp))) return bail(s);
-    cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key2.p, val.p, order.p, (int)n, 0, 32, st);
-  }
-  k_rank_inverse<<<grid_for(n), 256, 0, st>>>(n, order.p, g->off.p, rank.p, rdeg.p);
-  if ((s = scan_i64(n, rdeg.p, p->roff.p, st))) return bail(s);
-  {
-    DevBuf<int32_t> tmpadj;
-    if ((s = tmpadj.reserve(nnz))) return bail(s);
-    k_rank_copy<<<grid_for(n * 32), 256, 0, st>>>(n, order.p, rank.p, g->off.p, g->adj.p, p->roff.p, tmpadj.p);
-    size_t tmp = 0;
-    cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, tmpadj.p, p->radj.p, (int)nnz, (int)n, p->roff.p,
-                                       p->roff.p + 1, st);
-    DevBuf<char> t;
-    if ((s = t.reserve(tmp))) return bail(s);
-    cub::DeviceSegmentedSort::SortKeys(t.p, tmp, tmpadj.p, p->radj.p, (int)nnz, (int)n, p->roff.p,
-                                       p->roff.p + 1, st);
-  }
+  const int64_t *roff = g->rg->roff.p;
+  const int32_t *radj = g->rg->radj.p;
   // 2. owner / partner CSR
   DevBuf<int32_t> nshort;
   DevBuf<int64_t> tot;
@@ -426,11 +462,11 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
   cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(nshort.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
-  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, p->roff.p, p->radj.p, long_min, p->plong.p, nshort.p);
+  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, p->plong.p, nshort.p);
   k_partner_sizes<<<grid_for(n), 256, 0, st>>>(n, p->plong.p, nshort.p, tot.p);
   if ((s = scan_i64(n, tot.p, p->poff.p, st))) return bail(s);
   k_partner_cursors<<<grid_for(n), 256, 0, st>>>(n, p->poff.p, p->plong.p, curl.p, curs.p);
-  k_partner_fill<<<grid_for(n * 32), 256, 0, st>>>(n, p->roff.p, p->radj.p, long_min, curl.p, curs.p, p->padj.p,
+  k_partner_fill<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, curl.p, curs.p, p->padj.p,
                                                     work.p);
   // 3. task queues, heaviest first
   DevBuf<unsigned long long> ckey, wkey;
@@ -440,7 +476,7 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
       (s = sizes.reserve(2)) || (s = p->cta_tasks.reserve(n)) || (s = p->warp_tasks.reserve(n)))
     return bail(s);
   cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st);
-  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, p->roff.p, p->poff.p, work.p, cta_min, ckey.p, cval.p, wkey.p,
+  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->poff.p, work.p, cta_min, ckey.p, cval.p, wkey.p,
                                             wval.p, sizes.p);
   int h[2] = {0, 0};
   cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st);
@@ -473,7 +509,7 @@ int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
   GPM_TRY(rank_build_plan(g, 100, 32, st));
   RankPlan *p = g->rank;
   GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 4 * sizeof(int), st));
-  k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(p->roff.p, p->radj.p, p->poff.p, p->padj.p, p->plong.p,
+  k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->padj.p, p->plong.p,
                                                  p->cta_tasks.p, p->n_cta, p->warp_tasks.p, p->n_warp,
                                                  p->counters.p, d_out);
   GPM_LAUNCH_CHECK();

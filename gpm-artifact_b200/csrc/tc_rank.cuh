@@ -1,23 +1,35 @@
-// tc_rank.cuh -- plan of the rank-relabelled, smaller-side triangle count.
+// tc_rank.cuh -- rank-relabelled copy of a graph and the plan of the
+// smaller-side triangle count built on it.
 #pragma once
 #include "common.cuh"
 
 namespace gpm {
 
+// The stored graph renumbered by (in + out degree, id) rank, lists sorted.
+// upward == 1 when every stored edge points to a larger rank, which holds
+// for a degree-oriented DAG (orientation rule of graph.h:128-129); then
+// every out-list holds only ids above its owner.
+struct RankGraph {
+  DevBuf<int64_t> roff;   // n + 1
+  DevBuf<int32_t> radj;   // nnz
+  DevBuf<int32_t> order;  // rank -> original id
+  int upward = 0;
+};
+
 // Per-graph schedule of GPM_TC_BITMAP (device arrays):
-//   roff/radj   stored lists renumbered by (degree, id) rank, sorted
 //   poff/padj   partner CSR: for owner x, the vertices whose lists are
 //               streamed against N(x); the first plong[x] are long lists
 //   cta_tasks / warp_tasks  owners by size class, heaviest first
 struct RankPlan {
   int cta_min = 0, long_min = 0;
   int n_cta = 0, n_warp = 0;
-  DevBuf<int64_t> roff, poff;
-  DevBuf<int32_t> radj, padj, plong;
+  DevBuf<int64_t> poff;
+  DevBuf<int32_t> padj, plong;
   DevBuf<int32_t> cta_tasks, warp_tasks;
   DevBuf<int> counters;
 };
 
+int ensure_rank_graph(gpm_graph *g, cudaStream_t st);
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st);
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out);
 

@@ -1,0 +1,85 @@
+"""3/4-vertex motifs and the named patterns P1..P8 / Motif4 on the GPU vs the oracle."""
+import numpy as np
+import pytest
+
+import gpm
+import _oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def sym(n, s, d):
+    return orc.build_csr(n, s, d)
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_small_random_vs_bruteforce(seed):
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(5, 60))
+    e = rng.integers(0, n, size=(int(n * rng.uniform(1, 6)), 2)).astype(np.int32)
+    off, idx = sym(n, e[:, 0], e[:, 1])
+    bf = orc.bruteforce(off, idx)
+    g = gpm.Graph.from_edges(n, e[:, 0], e[:, 1])
+    assert g.motif(3).tolist() == bf[:2].tolist()
+    assert g.motif(4).tolist() == bf[2:].tolist()
+
+
+@pytest.mark.parametrize("gamma,mean,seed", [(2.1, 8.0, 1), (2.5, 16.0, 2), (2.8, 32.0, 3)])
+def test_chung_lu_vs_g2miner_restatement(gamma, mean, seed):
+    n, s, d = gpm.gen_chung_lu(3000, gamma, mean, seed=seed)
+    off, idx = sym(n, s, d)
+    doff, didx = orc.orient(off, idx)
+    g = gpm.Graph.from_edges(n, s, d)
+    assert g.motif(4).tolist() == orc.motif4(off, idx).tolist()
+    assert g.motif(3).tolist() == orc.motif3(off, idx, orc.tc(doff, didx)).tolist()
+
+
+def test_rmat_vs_g2miner_restatement():
+    n, s, d = gpm.gen_rmat(12, 16, seed=7)
+    off, idx = sym(n, s, d)
+    g = gpm.Graph.rmat(12, 16, seed=7)
+    assert g.motif(4).tolist() == orc.motif4(off, idx).tolist()
+
+
+def test_simple_mtx_fixture():
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_small.npz"))
+    e = z["simple_mtx"]
+    g = gpm.Graph.from_edges(4, e[:, 0], e[:, 1])
+    assert g.motif(4).tolist() == [0, 1, 0, 0, 0, 0]
+    assert g.motif(3).tolist() == [2, 0]
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("family", [gpm.G2MINER, gpm.PATTERN_SOLVER])
+def test_named_patterns(seed, family):
+    rng = np.random.default_rng(200 + seed)
+    n = int(rng.integers(20, 70))
+    e = rng.integers(0, n, size=(int(n * rng.uniform(2, 5)), 2)).astype(np.int32)
+    off, idx = sym(n, e[:, 0], e[:, 1])
+    g = gpm.Graph.from_edges(n, e[:, 0], e[:, 1])
+    for p in range(1, 9):
+        want = orc.pattern_g2miner(off, idx, p)
+        res, cnt = g.pattern(f"P{p}", family)
+        assert res == want, (p, res, want)
+        if family == gpm.PATTERN_SOLVER:
+            assert res == orc.pattern_solver(off, idx, p)[0]
+    res, cnt = g.pattern("Motif4", family)
+    m4 = orc.motif4(off, idx)
+    assert cnt.tolist() == m4.tolist()
+    assert res == (int(m4[0]) if family == gpm.G2MINER else (int(m4[1]) - int(m4[2])) % 2**64)
+
+
+def test_patterns_on_rmat():
+    n, s, d = gpm.gen_rmat(10, 8, seed=3)
+    off, idx = sym(n, s, d)
+    g = gpm.Graph.from_edges(n, s, d)
+    for p in (2, 3, 5, 6, 7, 8):
+        assert g.pattern(f"P{p}")[0] == orc.pattern_g2miner(off, idx, p, 0), p
+
+
+def test_unknown_pattern():
+    g = gpm.Graph.from_edges(3, [0, 1], [1, 2])
+    with pytest.raises(gpm.GpmError) as e:
+        g.pattern("P9")
+    assert e.value.status == 1
