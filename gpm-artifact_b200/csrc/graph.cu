@@ -560,6 +560,15 @@ int gpm_graph_orient(gpm_graph *g, int relabel) {
   return GPM_OK;
 }
 
+int gpm_graph_relabel(gpm_graph *g) {
+  if (!g) return fail(GPM_EINVAL, "NULL graph");
+  drop_plans(g);
+  GPM_TRY(relabel_device(g, 0));
+  GPM_TRY(compute_max_degree(g, 0));
+  GPM_CUDA(cudaDeviceSynchronize());
+  return GPM_OK;
+}
+
 int gpm_graph_work(gpm_graph *g, uint64_t *wedge_work, uint64_t *pair_work) {
   if (!g) return fail(GPM_EINVAL, "NULL graph");
   DevBuf<unsigned long long> o;

@@ -140,6 +140,8 @@ int gpm_graph_set_labels(gpm_graph *g, const int32_t *labels);
  * Graph::SortCSRGraph (graph.h:206-252): vertices renumbered by out-degree
  * descending (stable), lists re-sorted.  Runs on the device. */
 int gpm_graph_orient(gpm_graph *g, int relabel);
+/* Graph::SortCSRGraph (graph.h:206-252) alone, on the current lists. */
+int gpm_graph_relabel(gpm_graph *g);
 /* Algorithmic work figures of the (oriented) graph: *wedge_work =
  * sum over stored u->v of deg(v); *pair_work = sum over u->v of
  * (deg(u) + deg(v)). */
