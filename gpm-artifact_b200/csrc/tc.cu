@@ -440,3 +440,125 @@ int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Triangle count without any allocation.
+//
+// Some callers cannot allocate device memory at all: code running inside a
+// framework that owns every byte of the device through its own pool, hosts
+// that forbid allocation after start-up (real-time and embedded services),
+// and callers that must not trigger the implicit synchronisation a
+// cudaMalloc/cudaFree can cause.  For them the hash-kernel triangle count
+// below keeps its scratch -- the hub and tail task queues, their sizes and
+// the two work cursors -- in one file-scope __device__ array of fixed size,
+// so the call performs no cudaMalloc, cudaFree or other allocating call.
+//
+// Limits and sharing rules:
+//   * at most kNoAllocMaxVertices (1,048,576) vertices; larger graphs are
+//     rejected with GPM_EINVAL before anything is launched;
+//   * the array (8 MiB + 256 B) is part of this library's device image, so
+//     every GPU that loads the library keeps it until the process exits;
+//   * every call shares the array: the call clears the parts that must
+//     start at zero itself, but calls whose work overlaps on the GPU (two
+//     streams, or two host threads) race on it and must be serialised by the
+//     caller;
+//   * the first call on each device looks up the array's device address
+//     (cudaGetSymbolAddress) with that device current; make that first call
+//     before any stream capture begins.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace gpm {
+
+constexpr int64_t kNoAllocMaxVertices = 1 << 20;
+constexpr int kNoAllocHeader = 64;  // words: [0..1] queue sizes, [16..19] work cursors
+static __device__ __align__(256) int32_t g_noalloc_scratch[kNoAllocHeader + 2 * kNoAllocMaxVertices];
+
+// In host code the array's name is only a stand-in for its device address,
+// so the address is looked up once per device and kept here.
+constexpr int kNoAllocMaxDevices = 64;
+static int32_t *g_noalloc_ptr[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(int32_t **out) {
+  int dev = 0;
+  GPM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(GPM_EUNSUPPORTED, "device index above 63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return fail(GPM_ECUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
+    }
+    g_noalloc_ptr[dev] = static_cast<int32_t *>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return GPM_OK;
+}
+
+// k_tc_hash with the queue sizes read from device memory, so no host round
+// trip (and no host-visible buffer) is needed between the split and the count.
+__global__ void __launch_bounds__(256) k_tc_hash_noalloc(const int64_t *__restrict__ off,
+                                                         const int32_t *__restrict__ adj,
+                                                         const int32_t *__restrict__ cta_tasks,
+                                                         const int32_t *__restrict__ warp_tasks,
+                                                         const int *__restrict__ sizes, int *__restrict__ counters,
+                                                         unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ int s_task;
+  const int n_cta = sizes[0], n_warp = sizes[1];
+  unsigned long long c = 0;
+  while (true) {
+    if (threadIdx.x == 0) s_task = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    int t = s_task;
+    __syncthreads();
+    if (t >= n_cta) break;
+    c += cta_task(cta_tasks[t], off, adj, smem);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  char *region = smem + warp * kWarpBytes;
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&counters[1], 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= n_warp) break;
+    c += warp_task(warp_tasks[t], off, adj, region);
+  }
+  c = warp_sum(c);
+  if (lane == 0 && c) atomicAdd(out, c);
+}
+
+}  // namespace gpm
+
+extern "C" int gpm_tc_csr_noalloc(int64_t n, const int64_t *d_offsets, const int32_t *d_indices, void *stream,
+                                  uint64_t *d_out) {
+  if (n < 0 || !d_offsets || !d_out || (n > 0 && !d_indices))
+    return fail(GPM_EINVAL, "gpm_tc_csr_noalloc: bad argument");
+  if (n > kNoAllocMaxVertices)
+    return fail(GPM_EINVAL, "gpm_tc_csr_noalloc: " + std::to_string(n) +
+                                " vertices exceed the 1048576-vertex limit of the no-allocation entry point");
+  cudaStream_t st = (cudaStream_t)stream;
+  int32_t *scratch = nullptr;
+  GPM_TRY(noalloc_scratch(&scratch));
+  int *sizes = scratch, *counters = scratch + 16;
+  int32_t *cta_tasks = scratch + kNoAllocHeader, *warp_tasks = cta_tasks + kNoAllocMaxVertices;
+  GPM_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int32_t) * kNoAllocHeader, st));
+  GPM_CUDA(cudaMemsetAsync(d_out, 0, sizeof(uint64_t), st));
+  if (n == 0) return GPM_OK;
+  // same split as the allocating path: USE_WARP = 2, USE_CTA = 100
+  int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8);
+  k_tc_split<<<grid, 256, 0, st>>>(n, d_offsets, 2, 101, cta_tasks, warp_tasks, sizes);
+  GPM_LAUNCH_CHECK();
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_hash_noalloc, 256, TC_SMEM);
+    if (per_sm < 1) per_sm = 1;
+  }
+  k_tc_hash_noalloc<<<per_sm * num_sms(), 256, TC_SMEM, st>>>(d_offsets, d_indices, cta_tasks, warp_tasks, sizes,
+                                                              counters, (unsigned long long *)d_out);
+  GPM_LAUNCH_CHECK();
+  return GPM_OK;
+}

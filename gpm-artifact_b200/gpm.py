@@ -64,6 +64,7 @@ _SIGS = {
     "gpm_tc": ([_P, c_int, POINTER(c_uint64)], c_int),
     "gpm_tc_async": ([_P, c_int, _P, _P], c_int),
     "gpm_tc_host_csr": ([c_int64, _P, _P, c_int, _P, POINTER(c_uint64)], c_int),
+    "gpm_tc_csr_noalloc": ([c_int64, _P, _P, _P, _P], c_int),
     "gpm_clique": ([_P, c_int, POINTER(c_uint64)], c_int),
     "gpm_motif": ([_P, c_int, _P], c_int),
     "gpm_pattern": ([_P, c_char_p, c_int, _P, POINTER(c_uint64)], c_int),

@@ -164,6 +164,22 @@ int gpm_tc_async(gpm_graph *g, int variant, void *stream, uint64_t *d_out);
 int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, int variant,
                     void *stream, uint64_t *out);
 
+/* Triangle count of a device-resident CSR that allocates nothing -- this
+ * entry point has no counterpart in the reference.  It serves callers that
+ * cannot call cudaMalloc (a framework owning all device memory through its
+ * own pool, services that forbid allocation after start-up, code that must
+ * avoid the implicit synchronisation of allocation).  d_offsets[n+1] (int64)
+ * and d_indices (int32, sorted lists) are the caller's device arrays; the
+ * count (sum over stored u->v of |N(u) & N(v)|, the triangle count of a
+ * degree-oriented graph) is written to the caller's device uint64 d_out on
+ * `stream` without host synchronisation.  Scratch lives in a fixed 8 MiB
+ * array inside the library: at most 1,048,576 vertices (larger n is
+ * rejected with GPM_EINVAL); calls that overlap on the GPU race on that
+ * array; the first call on a device sets it up, so make it before any
+ * stream capture. */
+int gpm_tc_csr_noalloc(int64_t n, const int64_t *d_offsets, const int32_t *d_indices, void *stream,
+                       uint64_t *d_out);
+
 /* CFSolver (src/CFSolver.cuh:99-158): k-clique count on an oriented graph,
  * k in [3, 8]. */
 int gpm_clique(gpm_graph *g, int k, uint64_t *out);
