@@ -258,13 +258,14 @@ __global__ void __launch_bounds__(256) k_clique_local(int k, const int64_t *__re
   }
 }
 
-__global__ void k_clique_tasks(int64_t n, const int64_t *__restrict__ roff, int k, uint32_t *__restrict__ ckey,
+__global__ void k_clique_tasks(int64_t n, const int64_t *__restrict__ roff, int k, int warp_max,
+                               uint32_t *__restrict__ ckey,
                                int32_t *__restrict__ cval, uint32_t *__restrict__ wkey, int32_t *__restrict__ wval,
                                int *__restrict__ sizes) {
   for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
     int64_t d = roff[u + 1] - roff[u];
     if (d < k - 1) continue;
-    if (d > kCqWarpMax) {
+    if (d > warp_max) {
       int i = atomicAdd(&sizes[0], 1);
       ckey[i] = ~(uint32_t)d;
       cval[i] = (int32_t)u;
@@ -375,24 +376,35 @@ static int clique_local_grid() {
   return grid;
 }
 
-int clique_run_upward(int64_t n, const int64_t *roff, const int32_t *radj, int max_deg, int k, const int32_t *gid,
-                      unsigned long long *acc, int stride, int slot, cudaStream_t st) {
+// Plan: task queues (heaviest first) and row slabs; the run is launches only.
+int clique_plan_build(CliquePlan *p, int64_t n, const int64_t *roff, const int32_t *radj, int max_deg, int k,
+                      const int32_t *gid, unsigned long long *acc, int stride, int slot, cudaStream_t st,
+                      int warp_max) {
+  warp_max = std::max(1, std::min(warp_max, kCqWarpMax));
+  p->n = n;
+  p->roff = roff;
+  p->radj = radj;
+  p->k = k;
+  p->gid = gid;
+  p->acc = acc;
+  p->stride = stride;
+  p->slot = slot;
+  p->n_cta = p->n_warp = 0;
   if (n == 0) return GPM_OK;
   if (max_deg > kCqCtaMax) return fail(GPM_EUNSUPPORTED, "out-list longer than 2048 on the bitset clique path");
   DevBuf<uint32_t> ckey, wkey;
-  DevBuf<int32_t> cval, wval, ctasks, wtasks;
-  DevBuf<int> sizes, counters;
+  DevBuf<int32_t> cval, wval;
+  DevBuf<int> sizes;
   GPM_TRY(ckey.reserve(n));
   GPM_TRY(wkey.reserve(n));
   GPM_TRY(cval.reserve(n));
   GPM_TRY(wval.reserve(n));
-  GPM_TRY(ctasks.reserve(n));
-  GPM_TRY(wtasks.reserve(n));
+  GPM_TRY(p->ctasks.reserve(n));
+  GPM_TRY(p->wtasks.reserve(n));
   GPM_TRY(sizes.reserve(2));
-  GPM_TRY(counters.reserve(2));
+  GPM_TRY(p->counters.reserve(2));
   GPM_CUDA(cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st));
-  GPM_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(int), st));
-  k_clique_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, k, ckey.p, cval.p, wkey.p, wval.p, sizes.p);
+  k_clique_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, k, warp_max, ckey.p, cval.p, wkey.p, wval.p, sizes.p);
   int h[2];
   GPM_CUDA(cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st));
   GPM_CUDA(cudaStreamSynchronize(st));
@@ -403,22 +415,39 @@ int clique_run_upward(int64_t n, const int64_t *roff, const int32_t *radj, int m
     GPM_TRY(k2.reserve(cnt));
     size_t tmp = 0;
     uint32_t *kin = which ? wkey.p : ckey.p;
-    int32_t *vin = which ? wval.p : cval.p, *vout = which ? wtasks.p : ctasks.p;
+    int32_t *vin = which ? wval.p : cval.p, *vout = which ? p->wtasks.p : p->ctasks.p;
     GPM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kin, k2.p, vin, vout, cnt, 0, 32, st));
     DevBuf<char> t;
     GPM_TRY(t.reserve(tmp));
     GPM_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kin, k2.p, vin, vout, cnt, 0, 32, st));
   }
+  p->n_cta = h[0];
+  p->n_warp = h[1];
   // per-CTA slabs for rows that do not fit in shared memory
-  int grid = clique_local_grid();
+  p->grid = clique_local_grid();
   size_t W = (size_t)(max_deg + 31) / 32;
-  size_t slab_words = (size_t)max_deg * W * 4 + (size_t)max_deg * 4 > kCqSmem ? (size_t)max_deg * W : 1;
-  DevBuf<uint32_t> slabs;
-  GPM_TRY(slabs.reserve(slab_words * grid));
-  k_clique_local<<<grid, 256, kCqSmem, st>>>(k, roff, radj, ctasks.p, h[0], wtasks.p, h[1], counters.p, slabs.p,
-                                             slab_words, gid, acc, stride, slot);
+  p->slab_words = (size_t)max_deg * W * 4 + (size_t)max_deg * 4 > kCqSmem ? (size_t)max_deg * W : 1;
+  GPM_TRY(p->slabs.reserve(p->slab_words * p->grid));
+  GPM_CUDA(cudaStreamSynchronize(st));
+  return GPM_OK;
+}
+
+int clique_plan_run(CliquePlan *p, cudaStream_t st) {
+  if (p->n_cta + p->n_warp == 0) return GPM_OK;
+  GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 2 * sizeof(int), st));
+  k_clique_local<<<p->grid, 256, kCqSmem, st>>>(p->k, p->roff, p->radj, p->ctasks.p, p->n_cta, p->wtasks.p,
+                                                p->n_warp, p->counters.p, p->slabs.p, p->slab_words, p->gid, p->acc,
+                                                p->stride, p->slot);
   GPM_LAUNCH_CHECK();
-  GPM_CUDA(cudaStreamSynchronize(st));  // the scratch above is released on return
+  return GPM_OK;
+}
+
+int clique_run_upward(int64_t n, const int64_t *roff, const int32_t *radj, int max_deg, int k, const int32_t *gid,
+                      unsigned long long *acc, int stride, int slot, cudaStream_t st) {
+  CliquePlan p;
+  GPM_TRY(clique_plan_build(&p, n, roff, radj, max_deg, k, gid, acc, stride, slot, st));
+  GPM_TRY(clique_plan_run(&p, st));
+  GPM_CUDA(cudaStreamSynchronize(st));  // the plan's scratch is released on return
   return GPM_OK;
 }
 

@@ -210,7 +210,7 @@ __global__ void k_edge_sums(int64_t n, const int64_t *__restrict__ roff, const i
 constexpr int kC4WarpCap = 512;  // (key, count) slots per warp -> tasks with bound <= 256
 
 __global__ void k_c4_tasks(int64_t n, const int64_t *__restrict__ roff, const int64_t *__restrict__ split,
-                           const int32_t *__restrict__ radj, int32_t *__restrict__ cta_tasks,
+                           const int32_t *__restrict__ radj, int warp_bound, int32_t *__restrict__ cta_tasks,
                            int32_t *__restrict__ warp_tasks, int *__restrict__ sizes) {
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -223,7 +223,7 @@ __global__ void k_c4_tasks(int64_t n, const int64_t *__restrict__ roff, const in
     }
     b = warp_sum(b);
     if (lane == 0 && split[x] - roff[x] >= 2) {
-      if (b > (unsigned long long)(kC4WarpCap / 2)) cta_tasks[atomicAdd(&sizes[0], 1)] = (int32_t)x;
+      if (b > (unsigned long long)warp_bound) cta_tasks[atomicAdd(&sizes[0], 1)] = (int32_t)x;
       else warp_tasks[atomicAdd(&sizes[1], 1)] = (int32_t)x;
     }
   }
@@ -344,11 +344,12 @@ __global__ void k_up_copy(int64_t n, const int64_t *__restrict__ roff, const int
 }
 // tasks of the per-edge triangle pass: vertices with >= 2 upward neighbours
 __global__ void k_te_tasks(int64_t n, const int64_t *__restrict__ roff, const int64_t *__restrict__ split,
-                           int32_t *__restrict__ cta_tasks, int32_t *__restrict__ warp_tasks, int *__restrict__ sizes) {
+                           int cta_min, int32_t *__restrict__ cta_tasks, int32_t *__restrict__ warp_tasks,
+                           int *__restrict__ sizes) {
   for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
     int64_t d = roff[x + 1] - split[x];
     if (d < 2) continue;
-    if (d > kTeWarpCap / 2) cta_tasks[atomicAdd(&sizes[0], 1)] = (int32_t)x;
+    if (d > cta_min) cta_tasks[atomicAdd(&sizes[0], 1)] = (int32_t)x;
     else warp_tasks[atomicAdd(&sizes[1], 1)] = (int32_t)x;
   }
 }
@@ -387,77 +388,104 @@ static int dag_from_split(int64_t n, const int64_t *roff, const int64_t *split, 
   return GPM_OK;
 }
 
-int motif_pipeline(const MotifInput &in, cudaStream_t st, unsigned long long *d_acc, unsigned long long *d_out) {
+static int te_grid() {
+  static int grid = 0;
+  if (!grid) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edge_tri, 256, kTeSmem);
+    grid = std::max(1, per_sm) * num_sms();
+  }
+  return grid;
+}
+
+// Builds every schedule and scratch buffer of the pipeline (host syncs and
+// allocations happen here, never in motif_plan_run).
+int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
+  p->in = in;
   const int64_t n = in.n;
   const int64_t *roff = in.roff;
   const int32_t *radj = in.radj;
-  DevBuf<int64_t> split;
-  GPM_TRY(split.reserve(n));
-  GPM_CUDA(cudaMemsetAsync(d_acc, 0, sizeof(unsigned long long) * 8 * in.ngraphs, st));
-  if (n > 0) k_split<<<grid_for(n), 256, 0, st>>>(n, roff, radj, split.p);
-  // the upward parts as a CSR of their own: the DAG for the 4-cliques
-  DevBuf<int64_t> doff;
-  DevBuf<int32_t> dadj;
-  int dag_max = 0;
-  GPM_TRY(dag_from_split(n, roff, split.p, radj, doff, dadj, &dag_max, st));
-  // triangles per DAG edge, on the rank graph's upward parts
-  DevBuf<unsigned> te;
-  GPM_TRY(te.reserve(std::max<int64_t>(in.nnz, 1)));
-  GPM_CUDA(cudaMemsetAsync(te.p, 0, sizeof(unsigned) * std::max<int64_t>(in.nnz, 1), st));
-  {
-    DevBuf<int32_t> ct, wt;
-    DevBuf<int> sizes, counters;
-    GPM_TRY(ct.reserve(n));
-    GPM_TRY(wt.reserve(n));
-    GPM_TRY(sizes.reserve(2));
-    GPM_TRY(counters.reserve(2));
-    GPM_CUDA(cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st));
-    GPM_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(int), st));
-    if (n > 0) k_te_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, split.p, ct.p, wt.p, sizes.p);
-    int h[2];
-    GPM_CUDA(cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st));
-    GPM_CUDA(cudaStreamSynchronize(st));
-    static int grid = 0;
-    if (!grid) {
-      int per_sm = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edge_tri, 256, kTeSmem);
-      grid = std::max(1, per_sm) * num_sms();
-    }
-    if (h[0] + h[1] > 0)
-      k_edge_tri<<<grid, 256, kTeSmem, st>>>(roff, split.p, radj, ct.p, h[0], wt.p, h[1], counters.p, te.p);
-    GPM_LAUNCH_CHECK();
+  GPM_TRY(p->acc.reserve(8 * (size_t)in.ngraphs));
+  GPM_TRY(p->out.reserve(8 * (size_t)in.ngraphs));
+  GPM_TRY(p->split.reserve(n));
+  if (n > 0) k_split<<<grid_for(n), 256, 0, st>>>(n, roff, radj, p->split.p);
+  GPM_TRY(dag_from_split(n, roff, p->split.p, radj, p->doff, p->dadj, &p->dag_max, st));
+  GPM_TRY(p->te.reserve(std::max<int64_t>(in.nnz, 1)));
+  // queues of the per-edge triangle pass and of the 4-cycle pass
+  DevBuf<int> sizes;
+  GPM_TRY(sizes.reserve(4));
+  GPM_TRY(p->te_ct.reserve(n));
+  GPM_TRY(p->te_wt.reserve(n));
+  GPM_TRY(p->c4_ct.reserve(n));
+  GPM_TRY(p->c4_wt.reserve(n));
+  GPM_TRY(p->te_counters.reserve(2));
+  GPM_TRY(p->c4_counters.reserve(2));
+  GPM_CUDA(cudaMemsetAsync(sizes.p, 0, 4 * sizeof(int), st));
+  if (n > 0) {
+    k_te_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->split.p, std::min(in.te_cta_min, kTeWarpCap / 2), p->te_ct.p, p->te_wt.p, sizes.p);
+    k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, p->split.p, radj, std::min(in.c4_warp_bound, kC4WarpCap / 2), p->c4_ct.p, p->c4_wt.p, sizes.p + 2);
   }
-  if (n > 0) k_edge_sums<<<grid_for(n * 32), 256, 0, st>>>(n, roff, split.p, radj, te.p, in.gid, d_acc);
-  // 4-cycles
-  {
-    DevBuf<int32_t> ct, wt;
-    DevBuf<int> sizes, counters;
-    GPM_TRY(ct.reserve(n));
-    GPM_TRY(wt.reserve(n));
-    GPM_TRY(sizes.reserve(2));
-    GPM_TRY(counters.reserve(2));
-    GPM_CUDA(cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st));
-    GPM_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(int), st));
-    if (n > 0) k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, split.p, radj, ct.p, wt.p, sizes.p);
-    int h[2];
-    GPM_CUDA(cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st));
-    GPM_CUDA(cudaStreamSynchronize(st));
-    int grid = 2 * num_sms();
-    int64_t dense_len = std::max<int64_t>(in.max_graph_n, 1);
-    DevBuf<unsigned> dense;
-    GPM_TRY(dense.reserve((size_t)dense_len * grid));
-    GPM_CUDA(cudaMemsetAsync(dense.p, 0, sizeof(unsigned) * (size_t)dense_len * grid, st));
-    if (h[0] + h[1] > 0)
-      k_c4<<<grid, 256, 0, st>>>(roff, split.p, radj, in.gid, in.gbase, ct.p, h[0], wt.p, h[1], counters.p, dense.p,
-                                 dense_len, d_acc);
-    GPM_LAUNCH_CHECK();
-    GPM_CUDA(cudaStreamSynchronize(st));
-  }
-  // 4-cliques on the DAG (per graph)
-  GPM_TRY(clique_run_upward(n, doff.p, dadj.p, dag_max, 4, in.gid, d_acc, 8, 5, st));
-  k_motif_combine<<<std::max(1, (in.ngraphs + 255) / 256), 256, 0, st>>>(in.ngraphs, d_acc, d_out);
-  GPM_LAUNCH_CHECK();
+  int h[4];
+  GPM_CUDA(cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st));
   GPM_CUDA(cudaStreamSynchronize(st));
+  p->te_nc = h[0];
+  p->te_nw = h[1];
+  p->c4_nc = h[2];
+  p->c4_nw = h[3];
+  p->te_grid = te_grid();
+  p->c4_grid = 2 * num_sms();
+  // per-CTA dense 4-cycle counters over the largest member graph; kept zero
+  // between runs (the second pass of k_c4 clears what the first set)
+  p->dense_len = std::max<int64_t>(in.max_graph_n, 1);
+  GPM_TRY(p->dense.reserve((size_t)p->dense_len * p->c4_grid));
+  GPM_CUDA(cudaMemsetAsync(p->dense.p, 0, sizeof(unsigned) * (size_t)p->dense_len * p->c4_grid, st));
+  GPM_TRY(clique_plan_build(&p->k4, n, p->doff.p, p->dadj.p, p->dag_max, 4, in.gid, p->acc.p, 8, 5, st,
+                            in.cq_warp_max));
+  GPM_CUDA(cudaStreamSynchronize(st));
+  return GPM_OK;
+}
+
+// Launches only (capturable): zero the sums, triangles per edge, per-edge
+// and per-vertex sums, 4-cycles, 4-cliques, inversion.
+int motif_plan_run(MotifPlan *p, cudaStream_t st) {
+  const MotifInput &in = p->in;
+  const int64_t n = in.n;
+  GPM_CUDA(cudaMemsetAsync(p->acc.p, 0, sizeof(unsigned long long) * 8 * in.ngraphs, st));
+  GPM_CUDA(cudaMemsetAsync(p->te.p, 0, sizeof(unsigned) * std::max<int64_t>(in.nnz, 1), st));
+  GPM_CUDA(cudaMemsetAsync(p->te_counters.p, 0, 2 * sizeof(int), st));
+  GPM_CUDA(cudaMemsetAsync(p->c4_counters.p, 0, 2 * sizeof(int), st));
+  if (p->te_nc + p->te_nw > 0)
+    k_edge_tri<<<p->te_grid, 256, kTeSmem, st>>>(in.roff, p->split.p, in.radj, p->te_ct.p, p->te_nc, p->te_wt.p,
+                                                 p->te_nw, p->te_counters.p, p->te.p);
+  if (n > 0)
+    k_edge_sums<<<grid_for(n * 32), 256, 0, st>>>(n, in.roff, p->split.p, in.radj, p->te.p, in.gid, p->acc.p);
+  if (p->c4_nc + p->c4_nw > 0)
+    k_c4<<<p->c4_grid, 256, 0, st>>>(in.roff, p->split.p, in.radj, in.gid, in.gbase, p->c4_ct.p, p->c4_nc,
+                                     p->c4_wt.p, p->c4_nw, p->c4_counters.p, p->dense.p, p->dense_len, p->acc.p);
+  GPM_LAUNCH_CHECK();
+  GPM_TRY(clique_plan_run(&p->k4, st));
+  k_motif_combine<<<std::max(1, (in.ngraphs + 255) / 256), 256, 0, st>>>(in.ngraphs, p->acc.p, p->out.p);
+  GPM_LAUNCH_CHECK();
+  return GPM_OK;
+}
+
+int motif_plan_run_stage(MotifPlan *p, int stage, cudaStream_t st) {
+  const MotifInput &in = p->in;
+  if (stage == 0) {
+    GPM_CUDA(cudaMemsetAsync(p->te.p, 0, sizeof(unsigned) * std::max<int64_t>(in.nnz, 1), st));
+    GPM_CUDA(cudaMemsetAsync(p->te_counters.p, 0, 2 * sizeof(int), st));
+    if (p->te_nc + p->te_nw > 0)
+      k_edge_tri<<<p->te_grid, 256, kTeSmem, st>>>(in.roff, p->split.p, in.radj, p->te_ct.p, p->te_nc, p->te_wt.p,
+                                                   p->te_nw, p->te_counters.p, p->te.p);
+  } else if (stage == 1) {
+    GPM_CUDA(cudaMemsetAsync(p->c4_counters.p, 0, 2 * sizeof(int), st));
+    if (p->c4_nc + p->c4_nw > 0)
+      k_c4<<<p->c4_grid, 256, 0, st>>>(in.roff, p->split.p, in.radj, in.gid, in.gbase, p->c4_ct.p, p->c4_nc,
+                                       p->c4_wt.p, p->c4_nw, p->c4_counters.p, p->dense.p, p->dense_len, p->acc.p);
+  } else {
+    GPM_TRY(clique_plan_run(&p->k4, st));
+  }
+  GPM_LAUNCH_CHECK();
   return GPM_OK;
 }
 
@@ -476,12 +504,11 @@ extern "C" int gpm_motif(gpm_graph *g, int k, uint64_t *out) {
   in.roff = g->rg->roff.p;
   in.radj = g->rg->radj.p;
   in.max_graph_n = g->n;
-  DevBuf<unsigned long long> acc, res;
-  GPM_TRY(acc.reserve(8));
-  GPM_TRY(res.reserve(8));
-  GPM_TRY(motif_pipeline(in, 0, acc.p, res.p));
+  MotifPlan plan;
+  GPM_TRY(motif_plan_build(in, &plan, 0));
+  GPM_TRY(motif_plan_run(&plan, 0));
   unsigned long long h[8];
-  GPM_CUDA(cudaMemcpy(h, res.p, sizeof h, cudaMemcpyDeviceToHost));
+  GPM_CUDA(cudaMemcpy(h, plan.out.p, sizeof h, cudaMemcpyDeviceToHost));
   if (k == 3) {
     out[0] = h[0];
     out[1] = h[1];

@@ -210,7 +210,13 @@ __device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restric
   return c;
 }
 
-__global__ void __launch_bounds__(256) k_tc_rank(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+#ifndef GPM_TC_RANK_MIN_BLOCKS
+// CTAs per SM the register budget is sized for: 8 (32 registers) measured
+// 23.5 ms on R-MAT 22 against 25.5 ms at 6 and 29.3 ms at 4 (59 registers)
+#define GPM_TC_RANK_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
+    k_tc_rank(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
                                                  const int64_t *__restrict__ poff, const int32_t *__restrict__ padj,
                                                  const int32_t *__restrict__ plong,
                                                  const int32_t *__restrict__ cta_tasks, int n_cta,
@@ -246,10 +252,12 @@ __global__ void k_indeg(int64_t nnz, const int32_t *__restrict__ adj, int32_t *_
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x)
     atomicAdd(&indeg[adj[i]], 1);
 }
+// sort key: (graph id, in + out degree); the stable sort breaks ties by id
 __global__ void k_rank_keys(int64_t n, const int64_t *__restrict__ off, const int32_t *__restrict__ indeg,
-                            uint32_t *__restrict__ key, int32_t *__restrict__ val) {
+                            const int32_t *__restrict__ gid, uint64_t *__restrict__ key, int32_t *__restrict__ val) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    key[i] = (uint32_t)(off[i + 1] - off[i]) + (uint32_t)indeg[i];
+    uint64_t d = (uint64_t)(uint32_t)((off[i + 1] - off[i]) + indeg[i]);
+    key[i] = gid ? ((uint64_t)(uint32_t)gid[i] << 32) | d : d;
     val[i] = (int32_t)i;
   }
 }
@@ -379,7 +387,10 @@ __global__ void k_count_down(int64_t n, const int64_t *__restrict__ roff, const 
 void free_rank_graph(RankGraph *r) { delete r; }
 
 // Renumber the stored graph by (in + out degree, id) rank; lists re-sorted.
-int ensure_rank_graph(gpm_graph *g, cudaStream_t st) {
+// With a per-vertex graph id (a disjoint union of graphs whose vertices are
+// contiguous id ranges) the key is (graph id, degree), so every member graph
+// keeps its id range and is ranked within itself.
+int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid, int ngraphs) {
   if (g->rg) return GPM_OK;
   const int64_t n = g->n, nnz = g->nnz;
   RankGraph *r = new RankGraph();
@@ -389,7 +400,7 @@ int ensure_rank_graph(gpm_graph *g, cudaStream_t st) {
   };
   int s;
   DevBuf<int32_t> indeg, val, rank;
-  DevBuf<uint32_t> key, key2;
+  DevBuf<uint64_t> key, key2;
   DevBuf<int64_t> rdeg;
   DevBuf<int> down;
   if ((s = indeg.reserve(n)) || (s = val.reserve(n)) || (s = r->order.reserve(n)) || (s = rank.reserve(n)) ||
@@ -397,15 +408,18 @@ int ensure_rank_graph(gpm_graph *g, cudaStream_t st) {
       (s = r->radj.reserve(nnz)) || (s = down.reserve(1)))
     return bail(s);
   int32_t *order = r->order.p;
+  int end_bit = 32;
+  if (gid)
+    while (end_bit < 64 && (1ll << (end_bit - 32)) < ngraphs) ++end_bit;
   cudaMemsetAsync(indeg.p, 0, sizeof(int32_t) * n, st);
   k_indeg<<<grid_for(nnz), 256, 0, st>>>(nnz, g->adj.p, indeg.p);
-  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, indeg.p, key.p, val.p);
+  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, indeg.p, gid, key.p, val.p);
   {
     size_t tmp = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, val.p, order, (int)n, 0, 32, st);
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, val.p, order, (int)n, 0, end_bit, st);
     DevBuf<char> t;
     if ((s = t.reserve(tmp))) return bail(s);
-    cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key2.p, val.p, order, (int)n, 0, 32, st);
+    cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key2.p, val.p, order, (int)n, 0, end_bit, st);
   }
   k_rank_inverse<<<grid_for(n), 256, 0, st>>>(n, order, g->off.p, rank.p, rdeg.p);
   if ((s = scan_i64(n, rdeg.p, r->roff.p, st))) return bail(s);

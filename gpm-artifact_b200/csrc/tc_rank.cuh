@@ -29,7 +29,7 @@ struct RankPlan {
   DevBuf<int> counters;
 };
 
-int ensure_rank_graph(gpm_graph *g, cudaStream_t st);
+int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid = nullptr, int ngraphs = 1);
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st);
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out);
 

@@ -13,7 +13,7 @@ from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint6
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgpm.so")
+LIB_PATH = os.environ.get("GPM_LIB") or os.path.join(HERE, "libgpm.so")  # GPM_LIB: another build of it
 
 GPM_OK = 0
 STATUS = {0: "GPM_OK", 1: "GPM_EINVAL", 2: "GPM_ECUDA", 3: "GPM_ENOMEM", 4: "GPM_EUNSUPPORTED",
@@ -68,6 +68,14 @@ _SIGS = {
     "gpm_clique": ([_P, c_int, POINTER(c_uint64)], c_int),
     "gpm_motif": ([_P, c_int, _P], c_int),
     "gpm_pattern": ([_P, c_char_p, c_int, _P, POINTER(c_uint64)], c_int),
+    "gpm_batch_create": ([c_int, _P, _P, _P, _P, POINTER(c_void_p)], c_int),
+    "gpm_batch_generate_chung_lu": ([c_int, _P, _P, _P, c_uint64, POINTER(c_void_p)], c_int),
+    "gpm_batch_info": ([_P, POINTER(c_int), POINTER(c_int64), POINTER(c_int64)], c_int),
+    "gpm_batch_member_csr": ([_P, c_int, _P, _P, POINTER(c_int64), POINTER(c_int64)], c_int),
+    "gpm_batch_autotune": ([_P, _P], c_int),
+    "gpm_batch_motif": ([_P, c_int, _P, _P], c_int),
+    "gpm_batch_motif_async": ([_P, c_int, _P, _P], c_int),
+    "gpm_batch_destroy": ([_P], c_int),
     "gpm_query_create": ([c_int64, c_int64, _P, _P, _P, POINTER(c_void_p)], c_int),
     "gpm_query_destroy": ([_P], c_int),
     "gpm_match": ([_P, _P, POINTER(c_uint64)], c_int),
@@ -256,6 +264,67 @@ class Graph:
         out = c_uint64()
         check(lib.gpm_match(self.h, q.h, ctypes.byref(out)))
         return out.value
+
+
+class Batch:
+    """Owning wrapper of a gpm_batch (many graphs as one device union)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def from_edges(cls, members):
+        """members: list of (n, src, dst) with member-local ids."""
+        n = np.array([m[0] for m in members], np.int64)
+        m = np.array([len(x[1]) for x in members], np.int64)
+        src = _i32(np.concatenate([x[1] for x in members]) if len(members) else [])
+        dst = _i32(np.concatenate([x[2] for x in members]) if len(members) else [])
+        h = c_void_p()
+        check(lib.gpm_batch_create(len(members), _ptr(n), _ptr(m), _ptr(src), _ptr(dst), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def chung_lu(cls, n, gamma, mean_deg, seed=1):
+        n = np.ascontiguousarray(n, np.int64)
+        gm = np.ascontiguousarray(gamma, np.float64)
+        md = np.ascontiguousarray(mean_deg, np.float64)
+        h = c_void_p()
+        check(lib.gpm_batch_generate_chung_lu(len(n), _ptr(n), _ptr(gm), _ptr(md), seed, ctypes.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.gpm_batch_destroy(self.h)
+        self.h = None
+
+    __del__ = close
+
+    def info(self):
+        g, n, e = c_int(), c_int64(), c_int64()
+        check(lib.gpm_batch_info(self.h, ctypes.byref(g), ctypes.byref(n), ctypes.byref(e)))
+        return g.value, n.value, e.value
+
+    def member_csr(self, g):
+        n, e = c_int64(), c_int64()
+        check(lib.gpm_batch_member_csr(self.h, g, None, None, ctypes.byref(n), ctypes.byref(e)))
+        off = np.empty(n.value + 1, np.int64)
+        idx = np.empty(max(e.value, 1), np.int32)
+        check(lib.gpm_batch_member_csr(self.h, g, _ptr(off), _ptr(idx), ctypes.byref(n), ctypes.byref(e)))
+        return off, idx[: e.value]
+
+    def autotune(self):
+        t = np.zeros(3, np.int32)
+        check(lib.gpm_batch_autotune(self.h, _ptr(t)))
+        return t.tolist()
+
+    def motif(self, use_graph=True, stream_ptr=0):
+        ng = self.info()[0]
+        out = np.zeros(8 * ng, np.uint64)
+        check(lib.gpm_batch_motif(self.h, 1 if use_graph else 0, c_void_p(stream_ptr), _ptr(out)))
+        return out.reshape(ng, 8)
+
+    def motif_async(self, use_graph, stream_ptr, d_out_ptr):
+        check(lib.gpm_batch_motif_async(self.h, 1 if use_graph else 0, c_void_p(stream_ptr), c_void_p(d_out_ptr)))
 
 
 class Query:

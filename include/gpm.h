@@ -198,6 +198,36 @@ int gpm_motif(gpm_graph *g, int k, uint64_t *out);
 int gpm_pattern(gpm_graph *g, const char *name, int family, uint64_t *counters,
                 uint64_t *result);
 
+/* ---- batches of graphs (no reference counterpart: the reference runs one
+ * solver per graph and synchronises after every kernel,
+ * src/PatternSolver.cuh:177-246) ---------------------------------------------- */
+typedef struct gpm_batch gpm_batch;
+/* Many symmetric graphs held as one device-resident disjoint union.  Member g
+ * has n[g] vertices and m[g] undirected edges; src/dst hold all members'
+ * edges back to back with member-local ids. */
+int gpm_batch_create(int ngraphs, const int64_t *n, const int64_t *m, const int32_t *src, const int32_t *dst,
+                     gpm_batch **out);
+/* Seeded Chung-Lu members generated on the device (member g uses seed
+ * mix(seed + g), n[g] vertices, exponent gamma[g], mean degree mean_deg[g]). */
+int gpm_batch_generate_chung_lu(int ngraphs, const int64_t *n, const double *gamma, const double *mean_deg,
+                                uint64_t seed, gpm_batch **out);
+int gpm_batch_info(const gpm_batch *b, int *ngraphs, int64_t *n_total, int64_t *nnz_total);
+/* Member g's symmetric CSR (member-local ids); two-call pattern on NULL buffers. */
+int gpm_batch_member_csr(const gpm_batch *b, int g, int64_t *offsets, int32_t *indices, int64_t *n, int64_t *nnz);
+/* Chooses the pipeline's three task-split thresholds for this batch by
+ * timing candidates; tuned[3] (may be NULL) receives them. */
+int gpm_batch_autotune(gpm_batch *b, int *tuned);
+/* 3- and 4-vertex motifs of every member: out[8*g + i], i as in gpm_motif
+ * (0..1: induced 2-paths, triangles; 2..7: 3-star, 4-path, tailed triangle,
+ * 4-cycle, diamond, 4-clique).  One launch per pipeline stage covers all
+ * members; use_graph != 0 captures the stages into a CUDA graph on the first
+ * call and replays it afterwards. */
+int gpm_batch_motif(gpm_batch *b, int use_graph, void *stream, uint64_t *out);
+/* The same into device memory d_out (8 * ngraphs uint64) without host
+ * synchronisation; needs one gpm_batch_motif call before. */
+int gpm_batch_motif_async(gpm_batch *b, int use_graph, void *stream, uint64_t *d_out);
+int gpm_batch_destroy(gpm_batch *b);
+
 /* ---- labelled subgraph matching (sub_ceci semantics) ----------------------- */
 /* Query graph: n vertices (n <= 16), m undirected edges listed once, labels. */
 int gpm_query_create(int64_t n, int64_t m, const int32_t *src, const int32_t *dst,
