@@ -169,6 +169,8 @@ struct gpm_graph {
   gpm::TcPlan *tc = nullptr;    // cached triangle-count schedule (HASH)
   gpm::RankPlan *rank = nullptr; // cached schedule of the BITMAP path
   gpm::RankGraph *rg = nullptr;  // cached rank-relabelled copy
+  gpm::RankPlan *learned = nullptr;  // plan chosen by the attached scheduler
+  gpm_sched *sched = nullptr;        // learned scheduler (not owned)
   gpm::DevBuf<uint64_t> result; // small device result scratch
   ~gpm_graph();
 };

@@ -385,6 +385,8 @@ void drop_plans(gpm_graph *g) {
   g->rank = nullptr;
   free_rank_graph(g->rg);
   g->rg = nullptr;
+  free_rank_plan(g->learned);
+  g->learned = nullptr;
 }
 }  // namespace gpm
 

@@ -215,13 +215,16 @@ __device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restric
 // 23.5 ms on R-MAT 22 against 25.5 ms at 6 and 29.3 ms at 4 (59 registers)
 #define GPM_TC_RANK_MIN_BLOCKS 8
 #endif
+// REC = true is the instrumented build the learned scheduler trains on: it
+// logs each task's cost in warp-cycles (SM clock cycles x warps the task
+// occupied) into rec[owner].
+template <bool REC>
 __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
-    k_tc_rank(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                                                 const int64_t *__restrict__ poff, const int32_t *__restrict__ padj,
-                                                 const int32_t *__restrict__ plong,
-                                                 const int32_t *__restrict__ cta_tasks, int n_cta,
-                                                 const int32_t *__restrict__ warp_tasks, int n_warp,
-                                                 int *__restrict__ counters, unsigned long long *__restrict__ out) {
+    k_tc_rank_t(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+                const int64_t *__restrict__ poff, const int32_t *__restrict__ padj,
+                const int32_t *__restrict__ plong, const int32_t *__restrict__ cta_tasks, int n_cta,
+                const int32_t *__restrict__ warp_tasks, int n_warp, int *__restrict__ counters,
+                unsigned long long *__restrict__ out, unsigned long long *__restrict__ rec) {
   extern __shared__ __align__(16) uint32_t rsm[];
   __shared__ int s_task;
   unsigned long long c = 0;
@@ -231,7 +234,10 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     int t = s_task;
     __syncthreads();
     if (t >= n_cta) break;
-    c += rank_cta_task(cta_tasks[t], roff, radj, poff, padj, plong, rsm);
+    const int32_t x = cta_tasks[t];
+    long long t0 = REC ? clock64() : 0;
+    c += rank_cta_task(x, roff, radj, poff, padj, plong, rsm);
+    if (REC && threadIdx.x == 0) rec[x] = (unsigned long long)(clock64() - t0) * (blockDim.x >> 5);
   }
   const int wid = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31;
@@ -241,11 +247,15 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     if (lane == 0) t = atomicAdd(&counters[1], 1);
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= n_warp) break;
-    c += rank_warp_task(warp_tasks[t], roff, radj, poff, padj, plong, region);
+    const int32_t x = warp_tasks[t];
+    long long t0 = REC ? clock64() : 0;
+    c += rank_warp_task(x, roff, radj, poff, padj, plong, region);
+    if (REC && lane == 0) rec[x] = (unsigned long long)(clock64() - t0);
   }
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(out, c);
 }
+#define k_tc_rank k_tc_rank_t<false>
 
 // ------------------------------------------------------------ plan build
 __global__ void k_indeg(int64_t nnz, const int32_t *__restrict__ adj, int32_t *__restrict__ indeg) {
@@ -281,9 +291,17 @@ __global__ void k_rank_copy(int64_t n, const int32_t *__restrict__ order, const 
   }
 }
 
+// Per-owner task configuration (learned scheduler): queue = cfg / 3
+// (0 warp, 1 CTA), long-list threshold = kCfgLong[cfg % 3].
+__device__ __constant__ int kCfgLong[3] = {8, 32, 128};
+__device__ __forceinline__ int owner_long_min(const uint8_t *cfg, int32_t owner, int long_min) {
+  return cfg ? kCfgLong[cfg[owner] % 3] : long_min;
+}
+
 // owner/partner assignment of every stored edge; long = partner list length >= long_min
 __global__ void k_partner_count(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                                int long_min, int32_t *__restrict__ nlong, int32_t *__restrict__ nshort) {
+                                int long_min, const uint8_t *__restrict__ cfg, int32_t *__restrict__ nlong,
+                                int32_t *__restrict__ nshort) {
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = warp; u < n; u += nw) {
@@ -295,7 +313,7 @@ __global__ void k_partner_count(int64_t n, const int64_t *__restrict__ roff, con
       int32_t owner = own_u ? (int32_t)u : v;
       int64_t dp = own_u ? dv : du, dow = own_u ? du : dv;
       if (dow < 2) continue;
-      atomicAdd(dp >= long_min ? &nlong[owner] : &nshort[owner], 1);
+      atomicAdd(dp >= owner_long_min(cfg, owner, long_min) ? &nlong[owner] : &nshort[owner], 1);
     }
   }
 }
@@ -312,7 +330,7 @@ __global__ void k_partner_cursors(int64_t n, const int64_t *__restrict__ poff, c
   }
 }
 __global__ void k_partner_fill(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                               int long_min, unsigned long long *__restrict__ curl,
+                               int long_min, const uint8_t *__restrict__ cfg, unsigned long long *__restrict__ curl,
                                unsigned long long *__restrict__ curs, int32_t *__restrict__ padj,
                                unsigned long long *__restrict__ work) {
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -326,7 +344,8 @@ __global__ void k_partner_fill(int64_t n, const int64_t *__restrict__ roff, cons
       int32_t owner = own_u ? (int32_t)u : v, partner = own_u ? v : (int32_t)u;
       int64_t dp = own_u ? dv : du, dow = own_u ? du : dv;
       if (dow < 2) continue;
-      unsigned long long pos = atomicAdd(dp >= long_min ? &curl[owner] : &curs[owner], 1ull);
+      unsigned long long pos =
+          atomicAdd(dp >= owner_long_min(cfg, owner, long_min) ? &curl[owner] : &curs[owner], 1ull);
       padj[pos] = partner;
       atomicAdd(&work[owner], (unsigned long long)dp + 1ull);
     }
@@ -335,13 +354,13 @@ __global__ void k_partner_fill(int64_t n, const int64_t *__restrict__ roff, cons
 // tasks: owners with partners; key = ~work so an ascending sort puts heavy first
 __global__ void k_rank_tasks(int64_t n, const int64_t *__restrict__ roff, const int64_t *__restrict__ poff,
                              const unsigned long long *__restrict__ work, int cta_min,
-                             unsigned long long *__restrict__ ckey, int32_t *__restrict__ cval,
-                             unsigned long long *__restrict__ wkey, int32_t *__restrict__ wval,
-                             int *__restrict__ sizes) {
+                             const uint8_t *__restrict__ cfg, unsigned long long *__restrict__ ckey,
+                             int32_t *__restrict__ cval, unsigned long long *__restrict__ wkey,
+                             int32_t *__restrict__ wval, int *__restrict__ sizes) {
   for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
     if (poff[x + 1] == poff[x]) continue;
     int64_t d = roff[x + 1] - roff[x];
-    if (d > cta_min) {
+    if (cfg ? cfg[x] / 3 == 1 : d > cta_min) {
       int i = atomicAdd(&sizes[0], 1);
       ckey[i] = ~work[x];
       cval[i] = (int32_t)x;
@@ -451,6 +470,13 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
   if (g->rank && g->rank->cta_min == cta_min && g->rank->long_min == long_min) return GPM_OK;
   free_rank_plan(g->rank);
   g->rank = nullptr;
+  RankPlan *p = nullptr;
+  GPM_TRY(rank_plan_new(g, cta_min, long_min, nullptr, st, &p));
+  g->rank = p;
+  return GPM_OK;
+}
+
+int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, cudaStream_t st, RankPlan **out) {
   GPM_TRY(ensure_rank_graph(g, st));
   const int64_t n = g->n, nnz = g->nnz;
   RankPlan *p = new RankPlan();
@@ -476,11 +502,11 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
   cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(nshort.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
-  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, p->plong.p, nshort.p);
+  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, cfg, p->plong.p, nshort.p);
   k_partner_sizes<<<grid_for(n), 256, 0, st>>>(n, p->plong.p, nshort.p, tot.p);
   if ((s = scan_i64(n, tot.p, p->poff.p, st))) return bail(s);
   k_partner_cursors<<<grid_for(n), 256, 0, st>>>(n, p->poff.p, p->plong.p, curl.p, curs.p);
-  k_partner_fill<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, curl.p, curs.p, p->padj.p,
+  k_partner_fill<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, cfg, curl.p, curs.p, p->padj.p,
                                                     work.p);
   // 3. task queues, heaviest first
   DevBuf<unsigned long long> ckey, wkey;
@@ -490,7 +516,7 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
       (s = sizes.reserve(2)) || (s = p->cta_tasks.reserve(n)) || (s = p->warp_tasks.reserve(n)))
     return bail(s);
   cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st);
-  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->poff.p, work.p, cta_min, ckey.p, cval.p, wkey.p,
+  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->poff.p, work.p, cta_min, cfg, ckey.p, cval.p, wkey.p,
                                             wval.p, sizes.p);
   int h[2] = {0, 0};
   cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st);
@@ -502,7 +528,7 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
     return bail(s);
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank plan: ") + cudaGetErrorString(e)));
-  g->rank = p;
+  *out = p;
   return GPM_OK;
 }
 
@@ -516,18 +542,30 @@ static int rank_grid() {
   return grid;
 }
 
-int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
+// Launch of a given plan; rec != nullptr selects the instrumented build.
+int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long long *d_out,
+                     unsigned long long *rec) {
   GPM_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
   if (g->nnz == 0) return GPM_OK;
-  // reference-style fixed thresholds: owners with > 100 keys go to a CTA
-  GPM_TRY(rank_build_plan(g, 100, 32, st));
-  RankPlan *p = g->rank;
   GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 4 * sizeof(int), st));
-  k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->padj.p, p->plong.p,
-                                                 p->cta_tasks.p, p->n_cta, p->warp_tasks.p, p->n_warp,
-                                                 p->counters.p, d_out);
+  if (rec)
+    k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->padj.p,
+                                                           p->plong.p, p->cta_tasks.p, p->n_cta, p->warp_tasks.p,
+                                                           p->n_warp, p->counters.p, d_out, rec);
+  else
+    k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->padj.p, p->plong.p,
+                                                   p->cta_tasks.p, p->n_cta, p->warp_tasks.p, p->n_warp,
+                                                   p->counters.p, d_out, nullptr);
   GPM_LAUNCH_CHECK();
   return GPM_OK;
+}
+
+int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
+  if (g->nnz == 0) return cudaMemsetAsync(d_out, 0, 8, st) == cudaSuccess ? GPM_OK : GPM_ECUDA;
+  // reference-style fixed thresholds: owners with > 100 keys go to a CTA,
+  // lists of >= 32 ids are streamed by a whole warp
+  GPM_TRY(rank_build_plan(g, 100, 32, st));
+  return rank_plan_launch(g, g->rank, st, d_out, nullptr);
 }
 
 }  // namespace gpm

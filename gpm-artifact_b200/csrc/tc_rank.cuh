@@ -32,5 +32,12 @@ struct RankPlan {
 int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid = nullptr, int ngraphs = 1);
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st);
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out);
+// An uncached plan; cfg (device, one byte per vertex, may be nullptr) gives
+// each owner its queue (cfg / 3: 0 warp, 1 CTA) and long-list threshold
+// ({8, 32, 128}[cfg % 3]) instead of the fixed thresholds.
+int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, cudaStream_t st, RankPlan **out);
+// rec != nullptr: instrumented run logging each owner's cost (warp-cycles) to rec[owner]
+int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long long *d_out,
+                     unsigned long long *rec);
 
 }  // namespace gpm

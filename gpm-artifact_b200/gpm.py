@@ -68,6 +68,18 @@ _SIGS = {
     "gpm_clique": ([_P, c_int, POINTER(c_uint64)], c_int),
     "gpm_motif": ([_P, c_int, _P], c_int),
     "gpm_pattern": ([_P, c_char_p, c_int, _P, POINTER(c_uint64)], c_int),
+    "gpm_sched_create": ([c_uint64, POINTER(c_void_p)], c_int),
+    "gpm_sched_destroy": ([_P], c_int),
+    "gpm_sched_param_count": ([], c_int),
+    "gpm_sched_get_params": ([_P, _P], c_int),
+    "gpm_sched_set_params": ([_P, _P], c_int),
+    "gpm_sched_collect": ([_P, _P, POINTER(c_int64)], c_int),
+    "gpm_sched_dataset": ([_P, POINTER(c_int64), _P, _P], c_int),
+    "gpm_sched_grad": ([_P, c_int64, _P, _P, _P, POINTER(c_double)], c_int),
+    "gpm_sched_predict": ([_P, c_int64, _P, _P], c_int),
+    "gpm_sched_train": ([_P, c_int, ctypes.c_float, POINTER(c_double)], c_int),
+    "gpm_sched_attach": ([_P, _P], c_int),
+    "gpm_sched_assign": ([_P, _P, _P], c_int),
     "gpm_batch_create": ([c_int, _P, _P, _P, _P, POINTER(c_void_p)], c_int),
     "gpm_batch_generate_chung_lu": ([c_int, _P, _P, _P, c_uint64, POINTER(c_void_p)], c_int),
     "gpm_batch_info": ([_P, POINTER(c_int), POINTER(c_int64), POINTER(c_int64)], c_int),
@@ -264,6 +276,73 @@ class Graph:
         out = c_uint64()
         check(lib.gpm_match(self.h, q.h, ctypes.byref(out)))
         return out.value
+
+
+class Sched:
+    """Owning wrapper of the learned task scheduler (gpm_sched)."""
+
+    def __init__(self, seed=1):
+        h = c_void_p()
+        check(lib.gpm_sched_create(seed, ctypes.byref(h)))
+        self.h = h
+        self.nparams = lib.gpm_sched_param_count()
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.gpm_sched_destroy(self.h)
+        self.h = None
+
+    __del__ = close
+
+    def params(self):
+        p = np.empty(self.nparams, np.float32)
+        check(lib.gpm_sched_get_params(self.h, _ptr(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        check(lib.gpm_sched_set_params(self.h, _ptr(p)))
+
+    def collect(self, g: "Graph") -> int:
+        r = c_int64()
+        check(lib.gpm_sched_collect(self.h, g.h, ctypes.byref(r)))
+        return r.value
+
+    def dataset(self):
+        r = c_int64()
+        check(lib.gpm_sched_dataset(self.h, ctypes.byref(r), None, None))
+        X = np.empty((r.value, 8), np.float32)
+        Y = np.empty((r.value, 6), np.float32)
+        check(lib.gpm_sched_dataset(self.h, ctypes.byref(r), _ptr(X), _ptr(Y)))
+        return X, Y
+
+    def grad(self, X, T):
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        gr = np.empty(self.nparams, np.float32)
+        loss = c_double()
+        check(lib.gpm_sched_grad(self.h, len(X), _ptr(X), _ptr(T), _ptr(gr), ctypes.byref(loss)))
+        return loss.value, gr
+
+    def predict(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.empty((len(X), 6), np.float32)
+        check(lib.gpm_sched_predict(self.h, len(X), _ptr(X), _ptr(Y)))
+        return Y
+
+    def train(self, steps, lr=1e-2):
+        loss = c_double()
+        check(lib.gpm_sched_train(self.h, steps, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def attach(self, g: "Graph"):
+        check(lib.gpm_sched_attach(g.h, self.h))
+
+    def assign(self, g: "Graph"):
+        n = g.info().n
+        cfg = np.empty(n, np.uint8)
+        check(lib.gpm_sched_assign(self.h, g.h, _ptr(cfg)))
+        return cfg
 
 
 class Batch:

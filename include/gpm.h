@@ -64,6 +64,7 @@ enum {
 
 typedef struct gpm_graph gpm_graph;
 typedef struct gpm_query gpm_query;
+typedef struct gpm_sched gpm_sched;
 
 typedef struct {
   int64_t n;           /* vertices                                  */
@@ -197,6 +198,33 @@ int gpm_motif(gpm_graph *g, int k, uint64_t *out);
  * h_total[1] or h_total[1]-h_total[2] for PatternSolver). */
 int gpm_pattern(gpm_graph *g, const char *name, int family, uint64_t *counters,
                 uint64_t *result);
+
+/* ---- learned task scheduler (no reference counterpart; replaces the fixed
+ * thresholds USE_CTA / USE_WARP of src/gpu_kernels/tuning_schedules.cuh:196-197,
+ * which remain the default schedule and the yardstick of its regret) --------
+ * Each owner task of GPM_TC_BITMAP gets one of 6 configurations:
+ * queue (cfg / 3: 0 warp, 1 CTA) x long-list threshold ({8, 32, 128}[cfg % 3]).
+ * A 3-layer FP32 MLP (8 -> 32 -> 32 -> 6) predicts log2 warp-cycles of each
+ * configuration from 8 task features; counts never depend on the choice. */
+int gpm_sched_create(uint64_t seed, gpm_sched **out);
+int gpm_sched_destroy(gpm_sched *s);
+int gpm_sched_param_count(void);
+int gpm_sched_get_params(const gpm_sched *s, float *params);
+int gpm_sched_set_params(gpm_sched *s, const float *params);
+/* Runs every owner task of g (oriented) under the 6 configurations with the
+ * instrumented kernel and appends (features, log2 cost) rows to s. */
+int gpm_sched_collect(gpm_sched *s, gpm_graph *g, int64_t *rows_added);
+/* Copies the dataset out (X: rows x 8, Y: rows x 6); NULL buffers: count only. */
+int gpm_sched_dataset(const gpm_sched *s, int64_t *rows, float *X, float *Y);
+/* Mean squared error over finite targets and its gradient (host arrays). */
+int gpm_sched_grad(gpm_sched *s, int64_t N, const float *X, const float *T, float *grad, double *loss);
+int gpm_sched_predict(gpm_sched *s, int64_t N, const float *X, float *Y);
+/* Full-batch Adam steps on the collected dataset, trained on the device. */
+int gpm_sched_train(gpm_sched *s, int steps, float lr, double *final_loss);
+/* GPM_TC_LEARNED on g uses s from now on (s must outlive g's use of it). */
+int gpm_sched_attach(gpm_graph *g, gpm_sched *s);
+/* The configuration the scheduler gives each vertex's task (255: no task). */
+int gpm_sched_assign(gpm_sched *s, gpm_graph *g, uint8_t *cfg);
 
 /* ---- batches of graphs (no reference counterpart: the reference runs one
  * solver per graph and synchronises after every kernel,
