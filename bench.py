@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (22 is the headline workload)")
-    ap.add_argument("--variant", default="auto", choices=["auto", "bitmap", "hash", "bsearch", "merge", "learned"])
+    ap.add_argument("--variant", default="learned",
+                    choices=["auto", "bitmap", "hash", "bsearch", "merge", "learned"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample time")
@@ -145,6 +146,21 @@ def cpu_sample(doff, didx, m_und, seconds, threads):
                               f"in {t:.2f} s, scaled to the whole graph")
 
 
+def profiled_traffic(scale, variant):
+    """DRAM bytes per launch of the count kernel from the committed ncu
+    summary of this workload (profiles/k_tc_rank_rmat22.md), else None."""
+    if scale != SCALE or variant not in ("learned", "bitmap", "auto"):
+        return None
+    path = os.path.join(ROOT, "profiles", "k_tc_rank_rmat22.md")
+    if not os.path.exists(path):
+        return None
+    key = f"traffic_bytes_per_launch[{'learned' if variant == 'learned' else 'bitmap'}]:"
+    for line in open(path):
+        if line.strip().startswith(key):
+            return int(line.split(":")[1].strip())
+    return None
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -173,8 +189,13 @@ def main():
     n, m_und = inf.n, inf.nnz
     wedge, pair = g.work()
     bytes_alg = 4 * (n + 1) + 4 * m_und + 4 * wedge
-    variant = {"auto": gpm.TC_AUTO, "bitmap": gpm.TC_BITMAP, "hash": gpm.TC_HASH, "bsearch": gpm.TC_BSEARCH, "merge": gpm.TC_MERGE,
-               "learned": gpm.TC_LEARNED}[args.variant]
+    variants = {"auto": gpm.TC_AUTO, "bitmap": gpm.TC_BITMAP, "hash": gpm.TC_HASH, "bsearch": gpm.TC_BSEARCH,
+                "merge": gpm.TC_MERGE, "learned": gpm.TC_LEARNED}
+    variant = variants[args.variant]
+    # the shipped scheduler weights (trained on logged task costs of smaller
+    # R-MAT and Chung-Lu graphs, none of them this graph)
+    sched = gpm.Sched.pretrained()
+    sched.set_default()
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
     out = torch.zeros(1, dtype=torch.int64, device=dev)
@@ -216,6 +237,25 @@ def main():
         m_total = float(m_und)
     value = m_total / (ms_step / 1e3)
 
+    # ---- the other schedules on the same graph (outside the timed region)
+    others = {}
+    for name in ("bitmap", "hash"):
+        if name == args.variant:
+            continue
+        v = variants[name]
+        g.tc_async(v, sp, out.data_ptr())
+        torch.cuda.synchronize()
+        assert int(out.item()) == count, name
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            g.tc_async(v, sp, out.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        others[name] = round(e0.elapsed_time(e1) / 3, 3)
+    others[args.variant] = round(ms_step, 3)
+
     # ---- end to end through the C ABI from pinned host memory
     e2e = None
     if not args.no_e2e:
@@ -255,6 +295,7 @@ def main():
     hbm, peak_kind = peaks()
     avg_kernel_ms = sum(per) / len(per)
     achieved = bytes_alg / (avg_kernel_ms / 1e3) / 1e9
+    traffic = profiled_traffic(args.scale, args.variant)
     if rank == 0:
         line = {
             "metric": "triangle-count TEPS (R-MAT scale 22, exact uint64)",
@@ -265,15 +306,16 @@ def main():
                        "edge_factor": EF, "abcd": [A, B, C, round(1 - A - B - C, 2)], "seed": "1+rank",
                        "n": n, "m_undirected": m_und, "dag_max_outdeg": inf.max_degree,
                        "triangles": count, "variant": args.variant, "parallelism": f"replicas{world}",
-                       "l2": "inputs > L2 (DAG %.0f MB), no flush" % ((8 * (n + 1) + 4 * m_und) / 1e6)},
+                       "l2": "inputs > L2 (DAG %.0f MB), no flush" % ((8 * (n + 1) + 4 * m_und) / 1e6),
+                       "ms_per_count_by_schedule": others},
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": peak_kind,
-                         "traffic": None, "algorithmic_bytes": bytes_alg, "kernel_ms": avg_kernel_ms},
+                         "traffic": traffic, "algorithmic_bytes": bytes_alg, "kernel_ms": avg_kernel_ms},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
-            "gpu_launches": args.steps * (1 if variant in (gpm.TC_AUTO, gpm.TC_HASH, gpm.TC_BSEARCH, gpm.TC_MERGE)
-                                          else 3),
+            # one count kernel per step (k_tc_rank, or k_tc_hash / k_tc_bsearch / k_tc_merge)
+            "gpu_launches": args.steps,
         }
         print(json.dumps(line), flush=True)
     g.close()

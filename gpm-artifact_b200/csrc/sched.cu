@@ -248,8 +248,12 @@ static int all_tasks(gpm_graph *g, DevBuf<int32_t> &tasks, int *ntasks, cudaStre
   return GPM_OK;
 }
 
+static gpm_sched *g_default_sched = nullptr;
+
 int tc_learned_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
-  if (!g->sched) return fail(GPM_EUNSUPPORTED, "no trained scheduler attached (gpm_sched_attach)");
+  if (!g->sched) g->sched = g_default_sched;
+  if (!g->sched)
+    return fail(GPM_EUNSUPPORTED, "no trained scheduler attached (gpm_sched_attach / gpm_sched_set_default)");
   if (!g->learned) {
     DevBuf<int32_t> tasks;
     int nt = 0;
@@ -439,6 +443,12 @@ int gpm_sched_attach(gpm_graph *g, gpm_sched *s) {
   free_rank_plan(g->learned);
   g->learned = nullptr;
   g->sched = s;
+  return GPM_OK;
+}
+
+// Process-wide scheduler for graphs without an attached one (NULL clears it).
+int gpm_sched_set_default(gpm_sched *s) {
+  g_default_sched = s;
   return GPM_OK;
 }
 

@@ -79,6 +79,7 @@ _SIGS = {
     "gpm_sched_predict": ([_P, c_int64, _P, _P], c_int),
     "gpm_sched_train": ([_P, c_int, ctypes.c_float, POINTER(c_double)], c_int),
     "gpm_sched_attach": ([_P, _P], c_int),
+    "gpm_sched_set_default": ([_P], c_int),
     "gpm_sched_assign": ([_P, _P, _P], c_int),
     "gpm_batch_create": ([c_int, _P, _P, _P, _P, POINTER(c_void_p)], c_int),
     "gpm_batch_generate_chung_lu": ([c_int, _P, _P, _P, c_uint64, POINTER(c_void_p)], c_int),
@@ -281,11 +282,21 @@ class Graph:
 class Sched:
     """Owning wrapper of the learned task scheduler (gpm_sched)."""
 
+    # Parameters trained on logged task costs of R-MAT (scales 15-18) and
+    # Chung-Lu graphs; the training recipe is tests/test_sched_gpu.py's.
+    PRETRAINED = os.path.join(HERE, "sched_tc.f32")
+
     def __init__(self, seed=1):
         h = c_void_p()
         check(lib.gpm_sched_create(seed, ctypes.byref(h)))
         self.h = h
         self.nparams = lib.gpm_sched_param_count()
+
+    @classmethod
+    def pretrained(cls):
+        s = cls()
+        s.set_params(np.fromfile(cls.PRETRAINED, dtype=np.float32))
+        return s
 
     def close(self):
         if getattr(self, "h", None) and lib is not None:
@@ -337,6 +348,11 @@ class Sched:
 
     def attach(self, g: "Graph"):
         check(lib.gpm_sched_attach(g.h, self.h))
+
+    def set_default(self):
+        """Use this scheduler for every graph without an attached one (keep
+        the object alive meanwhile)."""
+        check(lib.gpm_sched_set_default(self.h))
 
     def assign(self, g: "Graph"):
         n = g.info().n

@@ -223,6 +223,9 @@ int gpm_sched_predict(gpm_sched *s, int64_t N, const float *X, float *Y);
 int gpm_sched_train(gpm_sched *s, int steps, float lr, double *final_loss);
 /* GPM_TC_LEARNED on g uses s from now on (s must outlive g's use of it). */
 int gpm_sched_attach(gpm_graph *g, gpm_sched *s);
+/* Scheduler used by GPM_TC_LEARNED on graphs without an attached one,
+ * including the temporary graph of gpm_tc_host_csr (NULL clears it). */
+int gpm_sched_set_default(gpm_sched *s);
 /* The configuration the scheduler gives each vertex's task (255: no task). */
 int gpm_sched_assign(gpm_sched *s, gpm_graph *g, uint8_t *cfg);
 
