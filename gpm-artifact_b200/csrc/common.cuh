@@ -38,30 +38,73 @@ int fail(int status, const std::string &msg);
 int ensure_device();
 
 // ---------------------------------------------------------------- device buffers
+// A per-thread pool of device blocks kept across calls.  While an ArenaScope
+// is alive on a thread, DevBuf allocations of that thread come from the pool
+// and go back to it when freed, so a repeated one-shot call (upload, prepare,
+// count, download) performs no cudaMalloc/cudaFree after the first.  Only
+// entry points that run all their work on one stream and synchronise it
+// before returning open a scope, so a block is never reused while an earlier
+// kernel still reads it.
+struct Arena;
+Arena *current_arena();
+void *arena_get(Arena *a, size_t bytes, size_t *cap);
+void arena_put(Arena *a, void *p, size_t cap);
+struct ArenaScope {
+  ArenaScope();
+  ~ArenaScope();
+  Arena *prev;
+};
+
 // Owning device allocation; move-only.
 template <typename T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  Arena *arena = nullptr;  // pool the block came from (nullptr: cudaMalloc)
+  size_t cap = 0;          // bytes of a pooled block
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
-  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n), arena(o.arena), cap(o.cap) {
+    o.p = nullptr;
+    o.n = 0;
+    o.arena = nullptr;
+  }
   DevBuf &operator=(DevBuf &&o) noexcept {
-    if (this != &o) { reset(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) {
+      reset();
+      p = o.p;
+      n = o.n;
+      arena = o.arena;
+      cap = o.cap;
+      o.p = nullptr;
+      o.n = 0;
+      o.arena = nullptr;
+    }
     return *this;
   }
   ~DevBuf() { reset(); }
   void reset() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (arena) arena_put(arena, p, cap);
+      else cudaFree(p);
+    }
     p = nullptr;
     n = 0;
+    arena = nullptr;
   }
   // Grows to at least count elements (contents not preserved).
   int reserve(size_t count) {
     if (count <= n && p) return GPM_OK;
     reset();
     size_t bytes = (count ? count : 1) * sizeof(T);
+    if (Arena *a = current_arena()) {
+      p = static_cast<T *>(arena_get(a, bytes, &cap));
+      if (!p) return fail(GPM_ENOMEM, "device pool allocation of " + std::to_string(bytes) + " B failed");
+      arena = a;
+      n = count ? count : 1;
+      return GPM_OK;
+    }
     cudaError_t e = cudaMalloc((void **)&p, bytes);
     if (e != cudaSuccess) {
       cudaGetLastError();

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <fstream>
 #include <limits>
+#include <map>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -25,6 +26,59 @@ int fail(int status, const std::string &msg) {
   g_last_error = msg;
   return status;
 }
+
+// ------------------------------------------------------------------ device pool
+struct Arena {
+  std::multimap<size_t, void *> free_blocks;  // size -> block
+  int device = -1;
+  ~Arena() {
+    for (auto &b : free_blocks) cudaFree(b.second);
+  }
+};
+
+static thread_local Arena *tl_active = nullptr;
+static thread_local Arena tl_arena;
+
+Arena *current_arena() { return tl_active; }
+
+void *arena_get(Arena *a, size_t bytes, size_t *cap) {
+  const size_t gran = (size_t)1 << 18;  // 256 KiB granules keep reuse likely
+  size_t want = (bytes + gran - 1) / gran * gran;
+  auto it = a->free_blocks.lower_bound(want);
+  if (it != a->free_blocks.end() && it->first <= 2 * want + ((size_t)8 << 20)) {
+    void *p = it->second;
+    *cap = it->first;
+    a->free_blocks.erase(it);
+    return p;
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    // give the cached blocks back and retry once
+    for (auto &b : a->free_blocks) cudaFree(b.second);
+    a->free_blocks.clear();
+    if (cudaMalloc(&p, want) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+  }
+  *cap = want;
+  return p;
+}
+
+void arena_put(Arena *a, void *p, size_t cap) { a->free_blocks.emplace(cap, p); }
+
+ArenaScope::ArenaScope() : prev(tl_active) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (tl_arena.device != dev) {  // blocks belong to one device
+    for (auto &b : tl_arena.free_blocks) cudaFree(b.second);
+    tl_arena.free_blocks.clear();
+    tl_arena.device = dev;
+  }
+  tl_active = &tl_arena;
+}
+ArenaScope::~ArenaScope() { tl_active = prev; }
 
 int ensure_device() {
   int n = 0;

@@ -422,6 +422,9 @@ int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, i
   cudaStream_t st = (cudaStream_t)stream;
   GPM_TRY(ensure_device());
   int64_t nnz = offsets[n];
+  // every buffer below comes from this thread's reusable device pool; all
+  // work runs on `st` and is synchronised before returning
+  ArenaScope pool;
   gpm_graph g;
   g.n = n;
   g.nnz = nnz;
@@ -429,9 +432,15 @@ int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, i
   GPM_TRY(g.adj.reserve(nnz));
   GPM_CUDA(cudaMemcpyAsync(g.off.p, offsets, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
   if (nnz > 0) GPM_CUDA(cudaMemcpyAsync(g.adj.p, indices, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
-  GPM_TRY(orient_on_stream(&g, st));
-  GPM_TRY(g.result.reserve(8));
   if (variant == GPM_TC_AUTO) variant = GPM_TC_BITMAP;
+  if (variant == GPM_TC_BITMAP || variant == GPM_TC_LEARNED) {
+    // orientation folded into the rank relabel (one pass instead of two)
+    GPM_TRY(ensure_rank_graph(&g, st, nullptr, 1, true));
+    g.oriented = 1;
+  } else {
+    GPM_TRY(orient_on_stream(&g, st));
+  }
+  GPM_TRY(g.result.reserve(8));
   if (variant == GPM_TC_LEARNED) GPM_TRY(tc_learned_launch(&g, st, (unsigned long long *)g.result.p));
   else GPM_TRY(tc_launch(&g, variant, st, (unsigned long long *)g.result.p));
   GPM_CUDA(cudaMemcpyAsync(out, g.result.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));

@@ -291,6 +291,41 @@ __global__ void k_rank_copy(int64_t n, const int32_t *__restrict__ order, const 
   }
 }
 
+// Orientation folded into the relabel: keep only neighbours of larger rank
+// (the degree-oriented DAG of a symmetric graph, graph.h:128-129).
+__global__ void k_rank_up_count(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ rank,
+                                const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                                int64_t *__restrict__ rdeg) {
+  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < n; r += nw) {
+    int32_t v = order[r];
+    int64_t c = 0;
+    for (int64_t k = off[v] + lane_id(); k < off[v + 1]; k += 32) c += rank[adj[k]] > (int32_t)r;
+    c = warp_sum(c);
+    if (lane_id() == 0) rdeg[r] = c;
+  }
+}
+__global__ void k_rank_up_copy(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ rank,
+                               const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                               const int64_t *__restrict__ roff, int32_t *__restrict__ out) {
+  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = lane_id();
+  for (int64_t r = warp; r < n; r += nw) {
+    int32_t v = order[r];
+    int64_t s = off[v], e = off[v + 1], w = roff[r];
+    for (int64_t base = s; base < e; base += 32) {
+      int64_t k = base + lane;
+      int32_t x = k < e ? rank[adj[k]] : -1;
+      bool keep = x > (int32_t)r;
+      unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) out[w + __popc(m & ((1u << lane) - 1u))] = x;
+      w += __popc(m);
+    }
+  }
+}
+
 // Per-owner task configuration (learned scheduler): queue = cfg / 3
 // (0 warp, 1 CTA), long-list threshold = kCfgLong[cfg % 3].
 __device__ __constant__ int kCfgLong[3] = {8, 32, 128};
@@ -409,9 +444,10 @@ void free_rank_graph(RankGraph *r) { delete r; }
 // With a per-vertex graph id (a disjoint union of graphs whose vertices are
 // contiguous id ranges) the key is (graph id, degree), so every member graph
 // keeps its id range and is ranked within itself.
-int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid, int ngraphs) {
+int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid, int ngraphs, bool upward_only) {
   if (g->rg) return GPM_OK;
-  const int64_t n = g->n, nnz = g->nnz;
+  const int64_t n = g->n;
+  int64_t nnz = g->nnz;
   RankGraph *r = new RankGraph();
   auto bail = [&](int s) {
     delete r;
@@ -441,11 +477,20 @@ int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid, int ngr
     cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key2.p, val.p, order, (int)n, 0, end_bit, st);
   }
   k_rank_inverse<<<grid_for(n), 256, 0, st>>>(n, order, g->off.p, rank.p, rdeg.p);
+  if (upward_only)
+    k_rank_up_count<<<grid_for(n * 32), 256, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, rdeg.p);
   if ((s = scan_i64(n, rdeg.p, r->roff.p, st))) return bail(s);
+  if (upward_only) {
+    cudaMemcpyAsync(&nnz, r->roff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+  }
   {
     DevBuf<int32_t> tmpadj;
     if ((s = tmpadj.reserve(nnz))) return bail(s);
-    k_rank_copy<<<grid_for(n * 32), 256, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, r->roff.p, tmpadj.p);
+    if (upward_only)
+      k_rank_up_copy<<<grid_for(n * 32), 256, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, r->roff.p, tmpadj.p);
+    else
+      k_rank_copy<<<grid_for(n * 32), 256, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, r->roff.p, tmpadj.p);
     size_t tmp = 0;
     cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, tmpadj.p, r->radj.p, (int)nnz, (int)n, r->roff.p,
                                        r->roff.p + 1, st);

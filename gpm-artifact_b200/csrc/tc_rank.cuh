@@ -29,7 +29,10 @@ struct RankPlan {
   DevBuf<int> counters;
 };
 
-int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid = nullptr, int ngraphs = 1);
+// upward_only: keep only neighbours of larger rank, i.e. orient a symmetric
+// graph and relabel it in one pass (the DAG's own id order is lost).
+int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid = nullptr, int ngraphs = 1,
+                      bool upward_only = false);
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st);
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out);
 // An uncached plan; cfg (device, one byte per vertex, may be nullptr) gives
