@@ -451,11 +451,11 @@ int clique_run_upward(int64_t n, const int64_t *roff, const int32_t *radj, int m
   return GPM_OK;
 }
 
-int clique_launch(gpm_graph *g, int k, cudaStream_t st, unsigned long long *d_out) {
+int clique_launch(gpm_graph *g, int k, cudaStream_t st, unsigned long long *d_out, bool edge_centric = false) {
   GPM_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
   if (g->nnz == 0) return GPM_OK;
   GPM_TRY(ensure_rank_graph(g, st));
-  if (g->rg->upward && g->max_deg <= kCqCtaMax)
+  if (!edge_centric && g->rg->upward && g->max_deg <= kCqCtaMax)
     return clique_run_upward(g->n, g->rg->roff.p, g->rg->radj.p, g->max_deg, k, nullptr, d_out, 0, 0, st);
   // edge-centric path on the stored graph
   GPM_TRY(ensure_src(g, st));
@@ -474,11 +474,14 @@ int clique_launch(gpm_graph *g, int k, cudaStream_t st, unsigned long long *d_ou
 
 using namespace gpm;
 
-extern "C" int gpm_clique(gpm_graph *g, int k, uint64_t *out) {
+extern "C" int gpm_clique_ex(gpm_graph *g, int k, int variant, uint64_t *out) {
   if (!g || !out) return fail(GPM_EINVAL, "gpm_clique: NULL argument");
   if (k < 3 || k > kCqMaxK) return fail(GPM_EUNSUPPORTED, "k-clique supports 3 <= k <= 8");
+  if (variant != GPM_CLIQUE_AUTO && variant != GPM_CLIQUE_EDGE) return fail(GPM_EINVAL, "unknown clique variant");
   GPM_TRY(g->result.reserve(8));
-  GPM_TRY(clique_launch(g, k, 0, (unsigned long long *)g->result.p));
+  GPM_TRY(clique_launch(g, k, 0, (unsigned long long *)g->result.p, variant == GPM_CLIQUE_EDGE));
   GPM_CUDA(cudaMemcpy(out, g->result.p, sizeof(uint64_t), cudaMemcpyDeviceToHost));
   return GPM_OK;
 }
+
+extern "C" int gpm_clique(gpm_graph *g, int k, uint64_t *out) { return gpm_clique_ex(g, k, GPM_CLIQUE_AUTO, out); }

@@ -66,6 +66,7 @@ _SIGS = {
     "gpm_tc_host_csr": ([c_int64, _P, _P, c_int, _P, POINTER(c_uint64)], c_int),
     "gpm_tc_csr_noalloc": ([c_int64, _P, _P, _P, _P], c_int),
     "gpm_clique": ([_P, c_int, POINTER(c_uint64)], c_int),
+    "gpm_clique_ex": ([_P, c_int, c_int, POINTER(c_uint64)], c_int),
     "gpm_motif": ([_P, c_int, _P], c_int),
     "gpm_pattern": ([_P, c_char_p, c_int, _P, POINTER(c_uint64)], c_int),
     "gpm_sched_create": ([c_uint64, POINTER(c_void_p)], c_int),
@@ -257,9 +258,9 @@ class Graph:
     def tc_async(self, variant, stream_ptr, d_out_ptr):
         check(lib.gpm_tc_async(self.h, variant, c_void_p(stream_ptr), c_void_p(d_out_ptr)))
 
-    def clique(self, k) -> int:
+    def clique(self, k, edge_centric=False) -> int:
         out = c_uint64()
-        check(lib.gpm_clique(self.h, k, ctypes.byref(out)))
+        check(lib.gpm_clique_ex(self.h, k, 1 if edge_centric else 0, ctypes.byref(out)))
         return out.value
 
     def motif(self, k):

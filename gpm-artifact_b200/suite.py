@@ -1,0 +1,193 @@
+"""Measurements of the engine's other workloads, each beside its plain path.
+
+    python gpm-artifact_b200/suite.py [--only er,clique,match,batch] [--quick]
+
+Prints one JSON line per workload:
+  er      triangle count, Erdos-Renyi G(16384, 131072 draws), degree-oriented
+  clique  4- and 5-cliques, R-MAT scale 20 (ef 16): local-bitset kernel vs the
+          edge-centric kernel shaped like the reference's clique_k_edge_warp
+  match   labelled matching with sub_ceci semantics, R-MAT with 8 Zipf(1.2)
+          labels, five queries (triangle, 4-cycle, diamond, house, 6-vertex
+          pyramid = apex over a 5-cycle) found by seeded random walks on the
+          data graph with the walked vertices' labels
+  batch   all 3- and 4-vertex motifs of 256 Chung-Lu graphs (n log-uniform in
+          [1e3, 1e6], exponent U[2.1, 2.8], mean degree U[8, 64]): one union,
+          one launch per stage, CUDA-graph replay, autotuned -- against one
+          gpm_motif call per graph
+Times are CUDA-event or synchronised wall times of the counting calls; graph
+generation and host copies are outside them unless named.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import gpm  # noqa: E402
+
+SHAPES = {
+    "triangle": (3, [(0, 1), (1, 2), (2, 0)]),
+    "cycle4": (4, [(0, 1), (1, 2), (2, 3), (3, 0)]),
+    "diamond": (4, [(0, 1), (0, 2), (0, 3), (1, 2), (2, 3)]),
+    "house": (5, [(0, 1), (0, 4), (1, 2), (1, 4), (2, 3), (3, 4)]),
+    "pyramid6": (6, [(0, 1), (0, 2), (0, 3), (0, 4), (0, 5), (1, 2), (2, 3), (3, 4), (4, 5), (5, 1)]),
+}
+
+
+def timed(fn, reps=1):
+    import torch
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(reps):
+        r = fn()
+    torch.cuda.synchronize()
+    return r, (time.perf_counter() - t) / reps
+
+
+def walk_query(off, idx, labels, shape, rng, tries=2000):
+    """An embedding of `shape` found by a seeded randomised walk (depth-first,
+    random neighbour order); returns the walked vertices' labels."""
+    k, edges = shape
+    adj = [set() for _ in range(k)]
+    for a, b in edges:
+        adj[a].add(b)
+        adj[b].add(a)
+    n = len(off) - 1
+    deg = np.diff(off)
+
+    def nbrs(v):
+        return idx[off[v]:off[v + 1]]
+
+    def has(a, b):
+        lst = nbrs(a)
+        i = np.searchsorted(lst, b)
+        return i < len(lst) and lst[i] == b
+
+    for _ in range(tries):
+        start = int(rng.integers(n))
+        if deg[start] < len(adj[0]):
+            continue
+        emb = [start]
+
+        def extend(i):
+            if i == k:
+                return True
+            parent = next(j for j in range(i) if j in adj[i])
+            cand = nbrs(emb[parent])
+            for v in rng.permutation(cand)[:64]:
+                v = int(v)
+                if v in emb or deg[v] < len(adj[i]):
+                    continue
+                if all(has(emb[j], v) for j in range(i) if j in adj[i]):
+                    emb.append(v)
+                    if extend(i + 1):
+                        return True
+                    emb.pop()
+            return False
+
+        if extend(1):
+            return labels[np.array(emb)]
+    raise RuntimeError("no embedding found")
+
+
+def run_er():
+    import torch
+    n, s, d = gpm.gen_er(16384, 131072, seed=1)
+    g = gpm.Graph.from_edges(n, s, d).orient()
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    sp = torch.cuda.current_stream().cuda_stream
+    res = {}
+    for name, v in (("bitmap", gpm.TC_BITMAP), ("hash", gpm.TC_HASH), ("bsearch", gpm.TC_BSEARCH)):
+        g.tc_async(v, sp, out.data_ptr())
+        _, t = timed(lambda: g.tc_async(v, sp, out.data_ptr()), 20)
+        res[name] = t * 1e3
+    m = g.info().nnz
+    return {"workload": "tc_er_16384_131072", "triangles": int(out.item()), "m": m,
+            "ms_per_count": res, "teps_bitmap": m / (res["bitmap"] / 1e3)}
+
+
+def run_clique(scale):
+    g = gpm.Graph.rmat(scale, 16, seed=1).orient()
+    res = {"workload": f"clique_rmat{scale}_ef16"}
+    for k in (4, 5):
+        g.clique(k)
+        c, t = timed(lambda: g.clique(k))
+        c2, t2 = timed(lambda: g.clique(k, edge_centric=True))
+        assert c == c2, (k, c, c2)
+        res[f"k{k}"] = {"cliques": c, "ms_bitset": t * 1e3, "ms_edge_centric": t2 * 1e3,
+                        "cliques_per_s": c / t, "speedup": t2 / t}
+    return res
+
+
+def run_match(scale, seed=3):
+    n, s, d = gpm.gen_rmat(scale, 16, seed=seed)
+    lab = gpm.gen_zipf_labels(n, 8, 1.2, seed=seed)
+    g = gpm.Graph.from_edges(n, s, d, labels=lab)
+    off, idx = g.csr()
+    rng = np.random.default_rng(seed)
+    res = {"workload": f"match_rmat{scale}_ef16_zipf8", "queries": {}}
+    for name, shape in SHAPES.items():
+        ql = walk_query(off, idx, lab, shape, rng)
+        e = np.array(shape[1], np.int32)
+        q = gpm.Query(shape[0], e[:, 0], e[:, 1], ql)
+        c, t = timed(lambda: g.match(q))
+        res["queries"][name] = {"labels": ql.tolist(), "matches": c, "ms": t * 1e3, "matches_per_s": c / t}
+    return res
+
+
+def batch_members(count, nmax, seed=5):
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(np.log(1e3), np.log(nmax), count)).astype(np.int64)
+    gam = rng.uniform(2.1, 2.8, count)
+    md = rng.uniform(8, 64, count)
+    return n, gam, md
+
+
+def run_batch(count, nmax):
+    n, gam, md = batch_members(count, nmax)
+    b = gpm.Batch.chung_lu(n, gam, md, seed=11)
+    ng, ntot, nnz = b.info()
+    r0, t_first = timed(lambda: b.motif(use_graph=True))
+    tuned = b.autotune()
+    r1, t_tuned_first = timed(lambda: b.motif(use_graph=True))
+    r2, t_replay = timed(lambda: b.motif(use_graph=True), 3)
+    assert (r0 == r1).all() and (r1 == r2).all()
+    # plain: one gpm_motif call per member graph (its own schedule, its syncs)
+    t_plain = 0.0
+    for i in range(ng):
+        off, idx = b.member_csr(i)
+        g = gpm.Graph.from_csr(off, idx)
+        m4, t = timed(lambda: g.motif(4))
+        t_plain += t
+        assert m4.tolist() == r2[i, 2:].tolist(), i
+        g.close()
+    total = int(r2.sum())
+    return {"workload": f"motif_batch_{count}_chunglu_nmax{int(nmax)}", "graphs": ng, "vertices": ntot,
+            "stored_edges": nnz, "motif_instances": total, "tuned_thresholds": tuned,
+            "s_batched_first_call": t_first, "s_batched_replay": t_replay, "s_plain_per_graph": t_plain,
+            "speedup_replay_vs_plain": t_plain / t_replay, "instances_per_s": total / t_replay}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", default="er,clique,match,batch")
+    ap.add_argument("--quick", action="store_true", help="smaller sizes for a smoke run")
+    a = ap.parse_args()
+    todo = a.only.split(",")
+    if "er" in todo:
+        print(json.dumps(run_er()), flush=True)
+    if "clique" in todo:
+        print(json.dumps(run_clique(16 if a.quick else 20)), flush=True)
+    if "match" in todo:
+        print(json.dumps(run_match(12 if a.quick else 16)), flush=True)
+    if "batch" in todo:
+        print(json.dumps(run_batch(32 if a.quick else 256, 3e4 if a.quick else 1e6)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -184,6 +184,12 @@ int gpm_tc_csr_noalloc(int64_t n, const int64_t *d_offsets, const int32_t *d_ind
 /* CFSolver (src/CFSolver.cuh:99-158): k-clique count on an oriented graph,
  * k in [3, 8]. */
 int gpm_clique(gpm_graph *g, int k, uint64_t *out);
+/* Same with an explicit kernel: GPM_CLIQUE_AUTO (local bitset DAG per vertex
+ * when the graph is a degree-oriented DAG) or GPM_CLIQUE_EDGE (warp per
+ * stored edge with materialised intersections, the shape of
+ * clique_4_edge_warp / clique_5_edge_warp). */
+enum { GPM_CLIQUE_AUTO = 0, GPM_CLIQUE_EDGE = 1 };
+int gpm_clique_ex(gpm_graph *g, int k, int variant, uint64_t *out);
 
 /* Motif counting on a symmetric graph.  k = 3: out[0] = induced 2-paths,
  * out[1] = triangles.  k = 4: out[0..5] = 3-star, 4-path, tailed triangle,
