@@ -194,6 +194,7 @@ __device__ __forceinline__ T warp_sum(T v) {
 struct TcPlan;
 struct RankPlan;
 struct RankGraph;
+struct LabelCsr;
 struct MotifPlan;
 
 }  // namespace gpm
@@ -213,6 +214,7 @@ struct gpm_graph {
   gpm::RankPlan *rank = nullptr; // cached schedule of the BITMAP path
   gpm::RankGraph *rg = nullptr;  // cached rank-relabelled copy
   gpm::RankPlan *learned = nullptr;  // plan chosen by the attached scheduler
+  gpm::LabelCsr *lcsr = nullptr;     // label-partitioned lists (matching)
   gpm_sched *sched = nullptr;        // learned scheduler (not owned)
   gpm::DevBuf<uint64_t> result; // small device result scratch
   ~gpm_graph();
@@ -227,6 +229,7 @@ int compute_max_degree(gpm_graph *g, cudaStream_t st);
 void free_tc_plan(TcPlan *p);
 void free_rank_plan(RankPlan *p);
 void free_rank_graph(RankGraph *r);
+void free_label_csr(LabelCsr *p);
 // Drops every cached schedule (after the stored graph changed).
 void drop_plans(gpm_graph *g);
 int num_sms();

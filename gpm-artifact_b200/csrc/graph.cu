@@ -387,6 +387,8 @@ void drop_plans(gpm_graph *g) {
   g->rg = nullptr;
   free_rank_plan(g->learned);
   g->learned = nullptr;
+  free_label_csr(g->lcsr);
+  g->lcsr = nullptr;
 }
 }  // namespace gpm
 
@@ -549,6 +551,8 @@ int gpm_graph_set_labels(gpm_graph *g, const int32_t *labels) {
   if (!g || !labels) return fail(GPM_EINVAL, "NULL argument");
   GPM_TRY(g->labels.reserve(g->n));
   if (g->n > 0) GPM_CUDA(cudaMemcpy(g->labels.p, labels, sizeof(int32_t) * g->n, cudaMemcpyHostToDevice));
+  free_label_csr(g->lcsr);  // the label partition follows the labels
+  g->lcsr = nullptr;
   return GPM_OK;
 }
 

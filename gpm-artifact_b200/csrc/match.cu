@@ -16,7 +16,10 @@
 // degree, injectivity and back-edges 32 at a time and compacted with ballots
 // into per-warp scratch; the last level is only counted.  Work is drained
 // from an atomic root cursor.
+#include <cub/cub.cuh>
+
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <vector>
 
@@ -54,9 +57,29 @@ __device__ __forceinline__ bool has_edge(const int64_t *__restrict__ off, const 
   return false;
 }
 
-__global__ void __launch_bounds__(256) k_match(QueryPlan q, int64_t n, const int64_t *__restrict__ off,
-                                               const int32_t *__restrict__ adj, const int32_t *__restrict__ labels,
-                                               int32_t *__restrict__ scratch, int64_t maxd, int *__restrict__ cursor,
+// [s, e): v's neighbours with label l inside its label-partitioned list,
+// relative to off[v].  L == 0: the lists are not partitioned (labels >= 64),
+// the whole list is scanned and the label test filters.
+__device__ __forceinline__ void seg_range(const int64_t *__restrict__ off, const int32_t *__restrict__ loff, int L,
+                                          int32_t v, int l, int64_t *s, int64_t *e) {
+  if (L == 0) {
+    *s = 0;
+    *e = off[v + 1] - off[v];
+  } else if (l < 0 || l >= L) {
+    *s = *e = 0;
+  } else {
+    *s = loff[(int64_t)v * (L + 1) + l];
+    *e = loff[(int64_t)v * (L + 1) + l + 1];
+  }
+}
+
+// n = number of (root, second vertex) pairs
+__global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restrict__ pairs, int64_t n,
+                                               const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                                               const int32_t *__restrict__ ladj, const int32_t *__restrict__ loff,
+                                               int L, const int32_t *__restrict__ labels,
+                                               int32_t *__restrict__ scratch, int64_t maxd,
+                                               unsigned long long *__restrict__ cursor,
                                                unsigned long long *__restrict__ out) {
   const unsigned lane = lane_id();
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -64,34 +87,35 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, int64_t n, const int
   int32_t emb[kMaxQ];
   int cur[kMaxQ], sz[kMaxQ];
   unsigned long long c = 0;
+  // tasks are the (root, second vertex) pairs: parallelism over edges, not
+  // roots, so a hub root's subtree is spread over many warps
   while (true) {
-    int64_t r = 0;
-    if (lane == 0) r = atomicAdd(cursor, 1);
+    unsigned long long r = 0;
+    if (lane == 0) r = atomicAdd(cursor, 1ull);
     r = __shfl_sync(0xffffffffu, r, 0);
-    if (r >= n) break;
-    const int32_t v0 = (int32_t)r;
-    if (labels[v0] != q.label[0] || off[v0 + 1] - off[v0] < q.mindeg[0]) continue;
-    if (q.n == 1) {
-      c += lane == 0;
-      continue;
-    }
-    emb[0] = v0;
-    int depth = 1;  // position being filled
+    if (r >= (unsigned long long)n) break;
+    const int2 pr = pairs[r];
+    emb[0] = pr.x;
+    emb[1] = pr.y;
+    int depth = 2;  // position being filled
     bool build = true;
-    while (depth >= 1) {
+    while (depth >= 2) {
       if (build) {
-        // candidates of position `depth`: neighbours of the parent's image
+        // candidates of position `depth`: the parent image's neighbours with
+        // the position's label (one segment of the label-partitioned list)
         const int32_t pv = emb[q.parent_pos[depth]];
-        const int64_t s = off[pv], e = off[pv + 1];
+        const int32_t *seg = ladj + off[pv];
+        int64_t s, e;
+        seg_range(off, loff, L, pv, q.label[depth], &s, &e);
         const bool last = depth == q.n - 1;
-        int32_t *L = lists + (int64_t)(depth - 1) * maxd;
+        int32_t *Lst = lists + (int64_t)(depth - 2) * maxd;
         int cnt = 0;
         for (int64_t base = s; base < e; base += 32) {
           int64_t i = base + lane;
           bool ok = false;
           int32_t x = 0;
           if (i < e) {
-            x = __ldg(adj + i);
+            x = __ldg(seg + i);
             ok = labels[x] == q.label[depth] && off[x + 1] - off[x] >= q.mindeg[depth];
             for (int j = 0; ok && j < depth; ++j) ok = emb[j] != x;
             uint32_t bm = q.back_pos[depth];
@@ -102,7 +126,7 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, int64_t n, const int
             }
           }
           unsigned m = __ballot_sync(0xffffffffu, ok);
-          if (!last && ok) L[cnt + __popc(m & ((1u << lane) - 1u))] = x;
+          if (!last && ok) Lst[cnt + __popc(m & ((1u << lane) - 1u))] = x;
           cnt += __popc(m);
         }
         __syncwarp();
@@ -120,13 +144,76 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, int64_t n, const int
         --depth;
         continue;
       }
-      emb[depth] = lists[(int64_t)(depth - 1) * maxd + cur[depth]++];
+      emb[depth] = lists[(int64_t)(depth - 2) * maxd + cur[depth]++];
       ++depth;
       build = true;
     }
   }
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(out, c);
+}
+
+// (root, second) pairs: a warp per root with the query root's label; the
+// second vertex comes from the root's segment of the second query vertex's
+// label.  count_only: the query has two vertices, so the pairs are the answer.
+__global__ void k_match_pairs(QueryPlan q, int64_t n, const int64_t *__restrict__ off,
+                              const int32_t *__restrict__ ladj, const int32_t *__restrict__ loff, int L,
+                              const int32_t *__restrict__ labels, int count_only, int2 *__restrict__ pairs,
+                              unsigned long long *__restrict__ npairs) {
+  const unsigned lane = lane_id();
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = warp; v < n; v += nw) {
+    if (labels[v] != q.label[0] || off[v + 1] - off[v] < q.mindeg[0]) continue;
+    const int32_t *seg = ladj + off[v];
+    int64_t s, e;
+    seg_range(off, loff, L, (int32_t)v, q.label[1], &s, &e);
+    for (int64_t base = s; base < e; base += 32) {
+      int64_t i = base + lane;
+      int32_t x = 0;
+      bool ok = false;
+      if (i < e) {
+        x = __ldg(seg + i);
+        ok = labels[x] == q.label[1] && off[x + 1] - off[x] >= q.mindeg[1];
+      }
+      unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (!m) continue;
+      unsigned long long at = 0;
+      if (lane == 0) at = atomicAdd(npairs, (unsigned long long)__popc(m));
+      at = __shfl_sync(0xffffffffu, at, 0);
+      if (!count_only && ok) pairs[at + __popc(m & ((1u << lane) - 1u))] = make_int2((int32_t)v, x);
+    }
+  }
+}
+
+// Label-partitioned copy of the lists: neighbours sorted by (label, id); loff
+// holds, per vertex, the L + 1 segment starts relative to off[v].
+__global__ void k_label_keys(int64_t nnz, const int32_t *__restrict__ adj, const int32_t *__restrict__ labels, int L,
+                             uint64_t *__restrict__ keys) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x) {
+    int32_t w = adj[i];
+    uint32_t l = L > 1 ? (uint32_t)labels[w] : 0u;
+    keys[i] = ((uint64_t)l << 32) | (uint32_t)w;
+  }
+}
+__global__ void k_label_offsets(int64_t n, const int64_t *__restrict__ off, const uint64_t *__restrict__ keys, int L,
+                                int32_t *__restrict__ ladj, int32_t *__restrict__ loff) {
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = lane_id();
+  for (int64_t v = warp; v < n; v += nw) {
+    const int64_t s = off[v], e = off[v + 1];
+    // segment start of label l = number of entries with label < l (sorted)
+    for (int l = lane; l <= L; l += 32) {
+      int64_t lo = s, hi = e;
+      while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)(keys[mid] >> 32) < l) lo = mid + 1; else hi = mid;
+      }
+      loff[v * (L + 1) + l] = (int32_t)(lo - s);
+    }
+    for (int64_t k = s + lane; k < e; k += 32) ladj[k] = (int32_t)(keys[k] & 0xffffffffu);
+  }
 }
 
 static int plan_query(const gpm_query *q, const std::vector<int64_t> &label_freq, QueryPlan *p) {
@@ -170,6 +257,63 @@ static int plan_query(const gpm_query *q, const std::vector<int64_t> &label_freq
       else p->back_pos[k] |= 1u << j;
     }
   }
+  return GPM_OK;
+}
+
+// Label-partitioned copy of a labelled graph's lists (cached per graph).
+struct LabelCsr {
+  int L = 0;  // partitions (max label + 1); 0: labels too wide, lists copied as they are
+  DevBuf<int32_t> ladj, loff;
+};
+void free_label_csr(LabelCsr *p) { delete p; }
+
+__global__ void k_label_range(int64_t n, const int32_t *__restrict__ labels, int *__restrict__ mm) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    atomicMax(&mm[0], labels[i]);
+    atomicMin(&mm[1], labels[i]);
+  }
+}
+
+static int ensure_label_csr(gpm_graph *g) {
+  if (g->lcsr) return GPM_OK;
+  const int64_t n = g->n, nnz = g->nnz;
+  LabelCsr *lc = new LabelCsr();
+  auto bail = [&](int s) {
+    delete lc;
+    return s;
+  };
+  int s;
+  DevBuf<int> mm;
+  if ((s = mm.reserve(2)) || (s = lc->ladj.reserve(nnz))) return bail(s);
+  int init[2] = {INT32_MIN, INT32_MAX}, h[2] = {0, 0};
+  cudaMemcpy(mm.p, init, sizeof init, cudaMemcpyHostToDevice);
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
+  if (n > 0) k_label_range<<<std::max(1, blocks), 256>>>(n, g->labels.p, mm.p);
+  cudaMemcpy(h, mm.p, sizeof h, cudaMemcpyDeviceToHost);
+  const int L = (n > 0 && h[1] >= 0 && h[0] < 64) ? h[0] + 1 : 0;
+  lc->L = L;
+  if (L == 0) {
+    if ((s = lc->loff.reserve(1))) return bail(s);
+    if (nnz > 0) cudaMemcpy(lc->ladj.p, g->adj.p, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice);
+  } else {
+    DevBuf<uint64_t> keys, sorted;
+    if ((s = lc->loff.reserve((size_t)n * (L + 1))) || (s = keys.reserve(nnz)) || (s = sorted.reserve(nnz)))
+      return bail(s);
+    if (nnz > 0) {
+      k_label_keys<<<(int)std::min<int64_t>((nnz + 255) / 256, num_sms() * 16), 256>>>(nnz, g->adj.p, g->labels.p, L,
+                                                                                      keys.p);
+      size_t tmp = 0;
+      cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, keys.p, sorted.p, (int)nnz, (int)n, g->off.p, g->off.p + 1);
+      DevBuf<char> t;
+      if ((s = t.reserve(tmp))) return bail(s);
+      cub::DeviceSegmentedSort::SortKeys(t.p, tmp, keys.p, sorted.p, (int)nnz, (int)n, g->off.p, g->off.p + 1);
+    }
+    k_label_offsets<<<(int)std::min<int64_t>((n * 32 + 255) / 256, num_sms() * 16), 256>>>(n, g->off.p, sorted.p, L,
+                                                                                          lc->ladj.p, lc->loff.p);
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("label partition: ") + cudaGetErrorString(e)));
+  g->lcsr = lc;
   return GPM_OK;
 }
 
@@ -236,22 +380,46 @@ int gpm_match(gpm_graph *g, const gpm_query *q, uint64_t *out) {
   }
   QueryPlan plan;
   GPM_TRY(plan_query(q, freq, &plan));
+  if (q->n == 1) {
+    *out = (uint64_t)(plan.label[0] >= 0 && plan.label[0] < maxl ? freq[plan.label[0]] : 0);
+    return GPM_OK;
+  }
+  GPM_TRY(ensure_label_csr(g));
+  LabelCsr *lc = g->lcsr;
   const int64_t maxd = std::max(1, g->max_deg);
+  const int blocks = (int)std::min<int64_t>((g->n * 32 + 255) / 256, (int64_t)num_sms() * 16);
+  DevBuf<unsigned long long> d, npairs;
+  GPM_TRY(d.reserve(1));
+  GPM_TRY(npairs.reserve(1));
+  GPM_CUDA(cudaMemset(npairs.p, 0, 8));
+  // (root, second vertex) pairs: counted, then materialised
+  k_match_pairs<<<blocks, 256>>>(plan, g->n, g->off.p, lc->ladj.p, lc->loff.p, lc->L, g->labels.p, 1, nullptr,
+                                 npairs.p);
+  GPM_LAUNCH_CHECK();
+  unsigned long long np = 0;
+  GPM_CUDA(cudaMemcpy(&np, npairs.p, 8, cudaMemcpyDeviceToHost));
+  if (q->n == 2 || np == 0) {
+    *out = np;
+    return GPM_OK;
+  }
+  DevBuf<int2> pairs;
+  GPM_TRY(pairs.reserve(np));
+  GPM_CUDA(cudaMemset(npairs.p, 0, 8));
+  k_match_pairs<<<blocks, 256>>>(plan, g->n, g->off.p, lc->ladj.p, lc->loff.p, lc->L, g->labels.p, 0, pairs.p,
+                                 npairs.p);
+  GPM_LAUNCH_CHECK();
   int64_t warps = (int64_t)num_sms() * 4 * 8;
   const int64_t cap_words = (int64_t)2 << 30;
   while (warps > 32 && warps * maxd * (kMaxQ - 1) > cap_words) warps >>= 1;
   DevBuf<int32_t> scratch;
-  DevBuf<int> cursor;
-  DevBuf<unsigned long long> d;
+  DevBuf<unsigned long long> cursor;
   GPM_TRY(scratch.reserve((size_t)(warps * maxd * (kMaxQ - 1))));
   GPM_TRY(cursor.reserve(1));
-  GPM_TRY(d.reserve(1));
-  GPM_CUDA(cudaMemset(cursor.p, 0, sizeof(int)));
+  GPM_CUDA(cudaMemset(cursor.p, 0, 8));
   GPM_CUDA(cudaMemset(d.p, 0, 8));
-  if (g->n > 0) {
-    k_match<<<(int)(warps / 8), 256>>>(plan, g->n, g->off.p, g->adj.p, g->labels.p, scratch.p, maxd, cursor.p, d.p);
-    GPM_LAUNCH_CHECK();
-  }
+  k_match<<<(int)(warps / 8), 256>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p, lc->loff.p, lc->L,
+                                     g->labels.p, scratch.p, maxd, cursor.p, d.p);
+  GPM_LAUNCH_CHECK();
   unsigned long long h = 0;
   GPM_CUDA(cudaMemcpy(&h, d.p, 8, cudaMemcpyDeviceToHost));
   *out = h;
