@@ -161,6 +161,20 @@ def profiled_traffic(scale, variant):
     return None
 
 
+def over_ranks(dist, dev, ms, edges):
+    """Whole-job figures from one rank's own: (max over ranks of the per-step
+    milliseconds, sum over ranks of the undirected edges counted per step).
+    With no process group the rank's own figures are the job's."""
+    if not dist:
+        return float(ms), float(edges)
+    import torch
+    tt = torch.tensor([float(ms)], dtype=torch.float64, device=dev)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    me = torch.tensor([float(edges)], dtype=torch.float64, device=dev)
+    dist.all_reduce(me, op=dist.ReduceOp.SUM)
+    return float(tt.item()), float(me.item())
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -225,16 +239,7 @@ def main():
     ms_total = t_all0.elapsed_time(t_all1)
     per = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     assert int(out.item()) == count, "count changed between steps"
-    ms_step = ms_total / args.steps
-    if dist:
-        tt = torch.tensor([ms_step], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_step = float(tt.item())
-        me = torch.tensor([float(m_und)], device=dev)
-        dist.all_reduce(me, op=dist.ReduceOp.SUM)
-        m_total = float(me.item())
-    else:
-        m_total = float(m_und)
+    ms_step, m_total = over_ranks(dist, dev, ms_total / args.steps, m_und)
     value = m_total / (ms_step / 1e3)
 
     # ---- the other schedules on the same graph (outside the timed region)
@@ -276,11 +281,7 @@ def main():
             gpm.tc_host_csr_ptrs(nn, hoff.data_ptr(), hidx.data_ptr(), variant, sp)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms_e2e = e0.elapsed_time(e1) / ks
-        if dist:
-            tt = torch.tensor([ms_e2e], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms_e2e = float(tt.item())
+        ms_e2e, _ = over_ranks(dist, dev, e0.elapsed_time(e1) / ks, m_und)
         e2e = {"value": m_total / (ms_e2e / 1e3), "unit": "TEPS", "ms_per_step": ms_e2e,
                "h2d_bytes_per_step": int(hoff.numel() * 8 + hidx.numel() * 4), "d2h_bytes_per_step": 8}
 

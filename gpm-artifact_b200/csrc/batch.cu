@@ -292,6 +292,24 @@ int gpm_batch_autotune(gpm_batch *b, int *tuned) {
   return GPM_OK;
 }
 
+int gpm_batch_stage_ms(gpm_batch *b, float *ms) {
+  if (!b || !ms) return fail(GPM_EINVAL, "NULL argument");
+  GPM_TRY(ensure_plan(b));
+  cudaEvent_t e0, e1;
+  GPM_CUDA(cudaEventCreate(&e0));
+  GPM_CUDA(cudaEventCreate(&e1));
+  for (int stage = 0; stage < 3; ++stage) {
+    GPM_CUDA(cudaEventRecord(e0, 0));
+    GPM_TRY(motif_plan_run_stage(b->plan, stage, 0));
+    GPM_CUDA(cudaEventRecord(e1, 0));
+    GPM_CUDA(cudaEventSynchronize(e1));
+    GPM_CUDA(cudaEventElapsedTime(&ms[stage], e0, e1));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return GPM_OK;
+}
+
 int gpm_batch_motif_async(gpm_batch *b, int use_graph, void *stream, uint64_t *d_out) {
   if (!b || !d_out) return fail(GPM_EINVAL, "gpm_batch_motif_async: NULL argument");
   cudaStream_t st = (cudaStream_t)stream;

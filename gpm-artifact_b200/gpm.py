@@ -87,6 +87,7 @@ _SIGS = {
     "gpm_batch_info": ([_P, POINTER(c_int), POINTER(c_int64), POINTER(c_int64)], c_int),
     "gpm_batch_member_csr": ([_P, c_int, _P, _P, POINTER(c_int64), POINTER(c_int64)], c_int),
     "gpm_batch_autotune": ([_P, _P], c_int),
+    "gpm_batch_stage_ms": ([_P, _P], c_int),
     "gpm_batch_motif": ([_P, c_int, _P, _P], c_int),
     "gpm_batch_motif_async": ([_P, c_int, _P, _P], c_int),
     "gpm_batch_destroy": ([_P], c_int),
@@ -412,6 +413,11 @@ class Batch:
         t = np.zeros(3, np.int32)
         check(lib.gpm_batch_autotune(self.h, _ptr(t)))
         return t.tolist()
+
+    def stage_ms(self):
+        ms = np.zeros(3, np.float32)
+        check(lib.gpm_batch_stage_ms(self.h, _ptr(ms)))
+        return {"triangles_per_edge": float(ms[0]), "four_cycles": float(ms[1]), "four_cliques": float(ms[2])}
 
     def motif(self, use_graph=True, stream_ptr=0):
         ng = self.info()[0]

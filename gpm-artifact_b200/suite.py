@@ -157,6 +157,7 @@ def run_batch(count, nmax):
     r1, t_tuned_first = timed(lambda: b.motif(use_graph=True))
     r2, t_replay = timed(lambda: b.motif(use_graph=True), 3)
     assert (r0 == r1).all() and (r1 == r2).all()
+    stages = b.stage_ms()
     # plain: one gpm_motif call per member graph (its own schedule, its syncs)
     t_plain = 0.0
     for i in range(ng):
@@ -168,7 +169,7 @@ def run_batch(count, nmax):
         g.close()
     total = int(r2.sum())
     return {"workload": f"motif_batch_{count}_chunglu_nmax{int(nmax)}", "graphs": ng, "vertices": ntot,
-            "stored_edges": nnz, "motif_instances": total, "tuned_thresholds": tuned,
+            "stored_edges": nnz, "motif_instances": total, "tuned_thresholds": tuned, "stage_ms": stages,
             "s_batched_first_call": t_first, "s_batched_replay": t_replay, "s_plain_per_graph": t_plain,
             "speedup_replay_vs_plain": t_plain / t_replay, "instances_per_s": total / t_replay}
 

@@ -254,6 +254,9 @@ int gpm_batch_member_csr(const gpm_batch *b, int g, int64_t *offsets, int32_t *i
 /* Chooses the pipeline's three task-split thresholds for this batch by
  * timing candidates; tuned[3] (may be NULL) receives them. */
 int gpm_batch_autotune(gpm_batch *b, int *tuned);
+/* Device time of the pipeline's three heavy stages run alone: ms[0] triangles
+ * per edge, ms[1] 4-cycles, ms[2] 4-cliques (CUDA events). */
+int gpm_batch_stage_ms(gpm_batch *b, float *ms);
 /* 3- and 4-vertex motifs of every member: out[8*g + i], i as in gpm_motif
  * (0..1: induced 2-paths, triangles; 2..7: 3-star, 4-path, tailed triangle,
  * 4-cycle, diamond, 4-clique).  One launch per pipeline stage covers all
