@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <cmath>
 #include <random>
+#include <mutex>
+#include <set>
 #include <vector>
 
 #include "common.cuh"
@@ -158,16 +160,16 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
 
 // ------------------------------------------------------------ features
 // Owner x (a task of the heuristic plan): 8 features from its key list and
-// its partner lists.  One warp per owner; lane 0 writes.
+// its partner segments.  One warp per owner; lane 0 writes.
 __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restrict__ roff,
                                                const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                                               const int32_t *__restrict__ padj, unsigned lane, float *f) {
+                                               const longlong2 *__restrict__ pseg, unsigned lane, float *f) {
   const int64_t d = roff[x + 1] - roff[x];
   unsigned long long work = 0;
   long long mx = 0, nlong = 0;
   for (int64_t j = poff[x] + lane; j < poff[x + 1]; j += 32) {
-    int32_t y = padj[j];
-    long long len = roff[y + 1] - roff[y];
+    const longlong2 sg = pseg[j];
+    long long len = sg.y - sg.x;
     work += (unsigned long long)len;
     mx = max(mx, len);
     nlong += len >= 32;
@@ -188,13 +190,13 @@ __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restr
 
 __global__ void k_features(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
                            const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                           const int32_t *__restrict__ padj, float *__restrict__ X) {
+                           const longlong2 *__restrict__ pseg, float *__restrict__ X) {
   const unsigned lane = lane_id();
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t t = warp; t < ntasks; t += nw) {
     float f[kIn];
-    owner_features(tasks[t], roff, radj, poff, padj, lane, f);
+    owner_features(tasks[t], roff, radj, poff, pseg, lane, f);
     if (lane == 0)
       for (int i = 0; i < kIn; ++i) X[t * kIn + i] = f[i];
   }
@@ -209,7 +211,7 @@ __global__ void k_gather_costs(const int32_t *__restrict__ tasks, int ntasks, co
 // Fused scheduler: features + MLP inference + argmin -> cfg[owner].
 __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ tasks, int ntasks,
                                                 const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                                                const int64_t *__restrict__ poff, const int32_t *__restrict__ padj,
+                                                const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
                                                 const float *__restrict__ w, uint8_t *__restrict__ cfg) {
   __shared__ float sw[kParams];
   for (int i = threadIdx.x; i < kParams; i += blockDim.x) sw[i] = w[i];
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ task
   for (int64_t t = warp; t < ntasks; t += nw) {
     float f[kIn];
     const int32_t x = tasks[t];
-    owner_features(x, roff, radj, poff, padj, lane, f);
+    owner_features(x, roff, radj, poff, pseg, lane, f);
     if (lane == 0) {
       float h1[kH], h2[kH], y[kOut];
       mlp_forward(sw, f, h1, h2, y);
@@ -248,13 +250,28 @@ static int all_tasks(gpm_graph *g, DevBuf<int32_t> &tasks, int *ntasks, cudaStre
   return GPM_OK;
 }
 
+// Live schedulers: a graph keeps a plain pointer to the one attached to it,
+// and the process keeps one default, so every use checks that the scheduler
+// still exists (destroying it clears the default).
+static std::mutex g_sched_mu;
+static std::set<gpm_sched *> g_sched_live;
 static gpm_sched *g_default_sched = nullptr;
 
+static bool sched_live(gpm_sched *s) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  return s && g_sched_live.count(s);
+}
+
 int tc_learned_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
-  if (!g->sched) g->sched = g_default_sched;
-  if (!g->sched)
-    return fail(GPM_EUNSUPPORTED, "no trained scheduler attached (gpm_sched_attach / gpm_sched_set_default)");
   if (!g->learned) {
+    gpm_sched *s = g->sched;
+    if (!s) {
+      std::lock_guard<std::mutex> lk(g_sched_mu);
+      s = g_default_sched;
+    }
+    if (!s)
+      return fail(GPM_EUNSUPPORTED, "no trained scheduler attached (gpm_sched_attach / gpm_sched_set_default)");
+    if (!sched_live(s)) return fail(GPM_EINVAL, "the graph's scheduler was destroyed");
     DevBuf<int32_t> tasks;
     int nt = 0;
     GPM_TRY(all_tasks(g, tasks, &nt, st));
@@ -265,7 +282,7 @@ int tc_learned_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) 
     RankPlan *h = g->rank;
     if (nt > 0)
       k_assign<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p,
-                                                         h->padj.p, g->sched->w.p, cfg.p);
+                                                         h->pseg.p, s->w.p, cfg.p);
     GPM_LAUNCH_CHECK();
     RankPlan *p = nullptr;
     GPM_TRY(rank_plan_new(g, 100, 32, cfg.p, st, &p));
@@ -302,11 +319,21 @@ int gpm_sched_create(uint64_t seed, gpm_sched **out) {
   cudaMemcpy(s->w.p, h.data(), sizeof(float) * kParams, cudaMemcpyHostToDevice);
   cudaMemset(s->m.p, 0, sizeof(float) * kParams);
   cudaMemset(s->v.p, 0, sizeof(float) * kParams);
+  {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    g_sched_live.insert(s);
+  }
   *out = s;
   return GPM_OK;
 }
 
 int gpm_sched_destroy(gpm_sched *s) {
+  if (!s) return GPM_OK;
+  {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    if (!g_sched_live.erase(s)) return fail(GPM_EINVAL, "gpm_sched_destroy: not a live scheduler");
+    if (g_default_sched == s) g_default_sched = nullptr;
+  }
   delete s;
   return GPM_OK;
 }
@@ -351,7 +378,7 @@ int gpm_sched_collect(gpm_sched *s, gpm_graph *g, int64_t *rows_added) {
   }
   RankPlan *h = g->rank;
   k_features<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p,
-                                                       h->padj.p, s->X.p + s->rows * kIn);
+                                                       h->pseg.p, s->X.p + s->rows * kIn);
   DevBuf<unsigned long long> rec, cnt;
   DevBuf<uint8_t> cfg;
   GPM_TRY(rec.reserve(g->n));
@@ -440,6 +467,7 @@ int gpm_sched_train(gpm_sched *s, int steps, float lr, double *final_loss) {
 // g's GPM_TC_LEARNED variant uses s (s must outlive g or be detached).
 int gpm_sched_attach(gpm_graph *g, gpm_sched *s) {
   if (!g) return fail(GPM_EINVAL, "NULL graph");
+  if (s && !sched_live(s)) return fail(GPM_EINVAL, "gpm_sched_attach: not a live scheduler");
   free_rank_plan(g->learned);
   g->learned = nullptr;
   g->sched = s;
@@ -448,6 +476,8 @@ int gpm_sched_attach(gpm_graph *g, gpm_sched *s) {
 
 // Process-wide scheduler for graphs without an attached one (NULL clears it).
 int gpm_sched_set_default(gpm_sched *s) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  if (s && !g_sched_live.count(s)) return fail(GPM_EINVAL, "gpm_sched_set_default: not a live scheduler");
   g_default_sched = s;
   return GPM_OK;
 }
@@ -463,7 +493,7 @@ int gpm_sched_assign(gpm_sched *s, gpm_graph *g, uint8_t *cfg) {
   GPM_CUDA(cudaMemset(d.p, 255, g->n));
   RankPlan *h = g->rank;
   if (nt > 0)
-    k_assign<<<blocks((int64_t)nt * 32), 256>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p, h->padj.p,
+    k_assign<<<blocks((int64_t)nt * 32), 256>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p, h->pseg.p,
                                                s->w.p, d.p);
   GPM_LAUNCH_CHECK();
   GPM_CUDA(cudaMemcpy(cfg, d.p, g->n, cudaMemcpyDeviceToHost));

@@ -46,13 +46,15 @@ static int grid_for(int64_t work, int block = 256) {
 }
 
 // ------------------------------------------------------------ membership
+// Every key handed to a table lies in [min N(owner), max N(owner)]: the plan
+// clipped the partner segments to that range, so the bitmap needs no range
+// check.
 struct BitTable {
   const uint32_t *bm;
   int32_t base;
-  uint32_t span;
   __device__ __forceinline__ unsigned hit(int32_t w) const {
     uint32_t o = (uint32_t)(w - base);
-    return o < span ? (bm[o >> 5] >> (o & 31)) & 1u : 0u;
+    return (bm[o >> 5] >> (o & 31)) & 1u;
   }
 };
 struct HashTable {
@@ -70,46 +72,52 @@ struct HashTable {
   }
 };
 
-// Stream one sorted list [s, e) with the whole warp: 16-byte loads for the
-// aligned body, scalar loads for the unaligned head and tail.
+// One segment of radj streamed by the whole warp, one key per lane per step
+// (each step one coalesced 128-byte row).  The loop bounds are the same for
+// every lane: full 128-key blocks with four loads in flight per lane, then at
+// most four single steps, so a segment of L keys takes ceil(L / 32) steps.
 template <class T>
-__device__ __forceinline__ unsigned long long warp_stream(const int32_t *__restrict__ adj, int64_t s,
-                                                          int64_t e, const T &t, unsigned lane) {
-  unsigned long long c = 0;
-  int64_t a = min((s + 3) & ~(int64_t)3, e);
-  if ((int64_t)lane < a - s) c += t.hit(__ldg(adj + s + lane));
-  int64_t nv = (e - a) >> 2;
-  const int4 *p = reinterpret_cast<const int4 *>(adj + a);
-#pragma unroll 2
-  for (int64_t i = lane; i < nv; i += 32) {
-    int4 q = __ldg(p + i);
-    c += t.hit(q.x) + t.hit(q.y) + t.hit(q.z) + t.hit(q.w);
+__device__ __forceinline__ unsigned warp_segment(const int32_t *__restrict__ radj, longlong2 sg, const T &t,
+                                                 unsigned lane) {
+  const int32_t *__restrict__ q = radj + sg.x;
+  const int len = (int)(sg.y - sg.x);
+  const int full = len & ~127;
+  unsigned c = 0;
+  int i = (int)lane;
+  for (; i < full; i += 128) {
+    const int32_t a = __ldg(q + i), b = __ldg(q + i + 32), d = __ldg(q + i + 64), e = __ldg(q + i + 96);
+    c += t.hit(a) + t.hit(b) + t.hit(d) + t.hit(e);
   }
-  int64_t tl = a + nv * 4;
-  if ((int64_t)lane < e - tl) c += t.hit(__ldg(adj + tl + lane));
+  for (; i < len; i += 32) c += t.hit(__ldg(q + i));
   return c;
 }
 
-// Partners [p0, p1) of one owner: the first nlong are long lists (whole
-// warp each), the rest short (8-lane groups).  `wid`/`nw` spread partners
-// over the warps of the executing group (1 warp for warp tasks, the CTA's
-// warps for CTA tasks).
+// Segments [p0, p1) of one owner: the first nlong are long (a whole warp
+// each, the next descriptor loaded while the current one streams), the rest
+// short (8-lane groups).  `wid`/`nw` spread segments over the warps of the
+// executing group (1 warp for warp tasks, the CTA's warps for CTA tasks).
 template <class T>
-__device__ __forceinline__ unsigned long long scan_partners(const int64_t *__restrict__ roff,
-                                                            const int32_t *__restrict__ radj,
-                                                            const int32_t *__restrict__ padj, int64_t p0,
-                                                            int64_t p1, int nlong, const T &t, int wid,
-                                                            int nw, unsigned lane) {
+__device__ __forceinline__ unsigned long long scan_segments(const int32_t *__restrict__ radj,
+                                                            const longlong2 *__restrict__ pseg, int64_t p0,
+                                                            int64_t p1, int nlong, const T &t, int wid, int nw,
+                                                            unsigned lane) {
   unsigned long long c = 0;
-  for (int64_t j = p0 + wid; j < p0 + nlong; j += nw) {
-    int32_t y = padj[j];
-    c += warp_stream(radj, roff[y], roff[y + 1], t, lane);
+  const int64_t pl = p0 + nlong;
+  int64_t j = p0 + wid;
+  if (j < pl) {
+    longlong2 nx = pseg[j];
+    for (; j < pl; j += nw) {
+      const longlong2 sg = nx;
+      if (j + nw < pl) nx = pseg[j + nw];
+      c += warp_segment(radj, sg, t, lane);
+    }
   }
   const unsigned grp = lane >> 3, gl = lane & 7;
-  for (int64_t j = p0 + nlong + wid * 4 + grp; j < p1; j += nw * 4) {
-    int32_t y = padj[j];
-    int64_t s = roff[y], e = roff[y + 1];
-    for (int64_t k = s + gl; k < e; k += 8) c += t.hit(__ldg(radj + k));
+  for (j = pl + wid * 4 + grp; j < p1; j += nw * 4) {
+    const longlong2 sg = pseg[j];
+    unsigned cs = 0;
+    for (int64_t k = sg.x + gl; k < sg.y; k += 8) cs += t.hit(__ldg(radj + k));
+    c += cs;
   }
   return c;
 }
@@ -119,7 +127,7 @@ __device__ __forceinline__ int ceil_log2i(int x) { return x <= 1 ? 0 : 32 - __cl
 // ------------------------------------------------------------ tasks
 __device__ unsigned long long rank_cta_task(int32_t x, const int64_t *__restrict__ roff,
                                             const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                                            const int32_t *__restrict__ padj, const int32_t *__restrict__ plong,
+                                            const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
                                             uint32_t *words) {
   const int tid = threadIdx.x, nthr = blockDim.x, wid = tid >> 5, nw = nthr >> 5;
   const unsigned lane = tid & 31;
@@ -139,8 +147,8 @@ __device__ unsigned long long rank_cta_task(int32_t x, const int64_t *__restrict
       atomicOr(&words[o >> 5], 1u << (o & 31));
     }
     __syncthreads();
-    BitTable t{words, kmin, (uint32_t)span};
-    c = scan_partners(roff, radj, padj, p0, p1, nl, t, wid, nw, lane);
+    BitTable t{words, kmin};
+    c = scan_segments(radj, pseg, p0, p1, nl, t, wid, nw, lane);
   } else {
     int32_t *tab = reinterpret_cast<int32_t *>(words);
     for (int t0 = 0; t0 < d; t0 += kCtaHashChunk) {
@@ -157,7 +165,7 @@ __device__ unsigned long long rank_cta_task(int32_t x, const int64_t *__restrict
       }
       __syncthreads();
       HashTable t{tab, logcap};
-      c += scan_partners(roff, radj, padj, p0, p1, nl, t, wid, nw, lane);
+      c += scan_segments(radj, pseg, p0, p1, nl, t, wid, nw, lane);
     }
   }
   __syncthreads();
@@ -166,7 +174,7 @@ __device__ unsigned long long rank_cta_task(int32_t x, const int64_t *__restrict
 
 __device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restrict__ roff,
                                              const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                                             const int32_t *__restrict__ padj, const int32_t *__restrict__ plong,
+                                             const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
                                              uint32_t *words) {
   const unsigned lane = lane_id();
   const int64_t s0 = roff[x];
@@ -185,8 +193,8 @@ __device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restric
       atomicOr(&words[o >> 5], 1u << (o & 31));
     }
     __syncwarp();
-    BitTable t{words, kmin, (uint32_t)span};
-    c = scan_partners(roff, radj, padj, p0, p1, nl, t, 0, 1, lane);
+    BitTable t{words, kmin};
+    c = scan_segments(radj, pseg, p0, p1, nl, t, 0, 1, lane);
   } else {
     int32_t *tab = reinterpret_cast<int32_t *>(words);
     for (int t0 = 0; t0 < d; t0 += kWarpHashChunk) {
@@ -203,7 +211,7 @@ __device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restric
       }
       __syncwarp();
       HashTable t{tab, logcap};
-      c += scan_partners(roff, radj, padj, p0, p1, nl, t, 0, 1, lane);
+      c += scan_segments(radj, pseg, p0, p1, nl, t, 0, 1, lane);
     }
   }
   __syncwarp();
@@ -221,7 +229,7 @@ __device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restric
 template <bool REC>
 __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     k_tc_rank_t(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                const int64_t *__restrict__ poff, const int32_t *__restrict__ padj,
+                const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
                 const int32_t *__restrict__ plong, const int32_t *__restrict__ cta_tasks, int n_cta,
                 const int32_t *__restrict__ warp_tasks, int n_warp, int *__restrict__ counters,
                 unsigned long long *__restrict__ out, unsigned long long *__restrict__ rec) {
@@ -236,7 +244,7 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     if (t >= n_cta) break;
     const int32_t x = cta_tasks[t];
     long long t0 = REC ? clock64() : 0;
-    c += rank_cta_task(x, roff, radj, poff, padj, plong, rsm);
+    c += rank_cta_task(x, roff, radj, poff, pseg, plong, rsm);
     if (REC && threadIdx.x == 0) rec[x] = (unsigned long long)(clock64() - t0) * (blockDim.x >> 5);
   }
   const int wid = threadIdx.x >> 5;
@@ -249,7 +257,7 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     if (t >= n_warp) break;
     const int32_t x = warp_tasks[t];
     long long t0 = REC ? clock64() : 0;
-    c += rank_warp_task(x, roff, radj, poff, padj, plong, region);
+    c += rank_warp_task(x, roff, radj, poff, pseg, plong, region);
     if (REC && lane == 0) rec[x] = (unsigned long long)(clock64() - t0);
   }
   c = warp_sum(c);
@@ -333,22 +341,57 @@ __device__ __forceinline__ int owner_long_min(const uint8_t *cfg, int32_t owner,
   return cfg ? kCfgLong[cfg[owner] % 3] : long_min;
 }
 
-// owner/partner assignment of every stored edge; long = partner list length >= long_min
+__device__ __forceinline__ int64_t lower_bound_key(const int32_t *__restrict__ a, int64_t lo, int64_t hi,
+                                                   int32_t key) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (__ldg(a + mid) < key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+__device__ __forceinline__ int64_t upper_bound_key(const int32_t *__restrict__ a, int64_t lo, int64_t hi,
+                                                   int32_t key) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (__ldg(a + mid) <= key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Stored edge k = (u, radj[k]): the endpoint with the longer list owns it
+// (ties to u), the other is its partner.  The segment is the part of the
+// partner's list inside [min, max] of the owner's list; its start and length
+// go to sstart[k] / slen[k] (length 0: nothing to stream, also when the
+// owner has fewer than 2 keys and so closes no triangle through the edge).
 __global__ void k_partner_count(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
                                 int long_min, const uint8_t *__restrict__ cfg, int32_t *__restrict__ nlong,
-                                int32_t *__restrict__ nshort) {
+                                int32_t *__restrict__ nshort, int64_t *__restrict__ sstart,
+                                int32_t *__restrict__ slen) {
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = warp; u < n; u += nw) {
     int64_t s = roff[u], e = roff[u + 1], du = e - s;
     for (int64_t k = s + lane_id(); k < e; k += 32) {
       int32_t v = radj[k];
-      int64_t dv = roff[v + 1] - roff[v];
+      int64_t vs = roff[v], ve = roff[v + 1], dv = ve - vs;
       bool own_u = dv <= du;
       int32_t owner = own_u ? (int32_t)u : v;
-      int64_t dp = own_u ? dv : du, dow = own_u ? du : dv;
-      if (dow < 2) continue;
-      atomicAdd(dp >= owner_long_min(cfg, owner, long_min) ? &nlong[owner] : &nshort[owner], 1);
+      int64_t os = own_u ? s : vs, oe = own_u ? e : ve;
+      int64_t ps = own_u ? vs : s, pe = own_u ? ve : e;
+      int64_t lo = 0, len = 0;
+      if (oe - os >= 2) {
+        lo = lower_bound_key(radj, ps, pe, radj[os]);
+        len = upper_bound_key(radj, lo, pe, radj[oe - 1]) - lo;
+      }
+      sstart[k] = lo;
+      slen[k] = (int32_t)len;
+      if (len > 0) atomicAdd(len >= owner_long_min(cfg, owner, long_min) ? &nlong[owner] : &nshort[owner], 1);
     }
   }
 }
@@ -365,24 +408,24 @@ __global__ void k_partner_cursors(int64_t n, const int64_t *__restrict__ poff, c
   }
 }
 __global__ void k_partner_fill(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                               int long_min, const uint8_t *__restrict__ cfg, unsigned long long *__restrict__ curl,
-                               unsigned long long *__restrict__ curs, int32_t *__restrict__ padj,
+                               int long_min, const uint8_t *__restrict__ cfg, const int64_t *__restrict__ sstart,
+                               const int32_t *__restrict__ slen, unsigned long long *__restrict__ curl,
+                               unsigned long long *__restrict__ curs, longlong2 *__restrict__ pseg,
                                unsigned long long *__restrict__ work) {
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = warp; u < n; u += nw) {
     int64_t s = roff[u], e = roff[u + 1], du = e - s;
     for (int64_t k = s + lane_id(); k < e; k += 32) {
+      const int32_t len = slen[k];
+      if (len == 0) continue;
       int32_t v = radj[k];
-      int64_t dv = roff[v + 1] - roff[v];
-      bool own_u = dv <= du;
-      int32_t owner = own_u ? (int32_t)u : v, partner = own_u ? v : (int32_t)u;
-      int64_t dp = own_u ? dv : du, dow = own_u ? du : dv;
-      if (dow < 2) continue;
+      int32_t owner = roff[v + 1] - roff[v] <= du ? (int32_t)u : v;
       unsigned long long pos =
-          atomicAdd(dp >= owner_long_min(cfg, owner, long_min) ? &curl[owner] : &curs[owner], 1ull);
-      padj[pos] = partner;
-      atomicAdd(&work[owner], (unsigned long long)dp + 1ull);
+          atomicAdd(len >= owner_long_min(cfg, owner, long_min) ? &curl[owner] : &curs[owner], 1ull);
+      const int64_t lo = sstart[k];
+      pseg[pos] = make_longlong2(lo, lo + len);
+      atomicAdd(&work[owner], (unsigned long long)len + 1ull);
     }
   }
 }
@@ -532,27 +575,28 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
     return s;
   };
   int s;
-  if ((s = p->poff.reserve(n + 1)) || (s = p->padj.reserve(nnz)) || (s = p->plong.reserve(n)) ||
+  if ((s = p->poff.reserve(n + 1)) || (s = p->pseg.reserve(nnz)) || (s = p->plong.reserve(n)) ||
       (s = p->counters.reserve(4)))
     return bail(s);
   const int64_t *roff = g->rg->roff.p;
   const int32_t *radj = g->rg->radj.p;
-  // 2. owner / partner CSR
-  DevBuf<int32_t> nshort;
-  DevBuf<int64_t> tot;
+  // 2. owner / segment CSR
+  DevBuf<int32_t> nshort, slen;
+  DevBuf<int64_t> tot, sstart;
   DevBuf<unsigned long long> curl, curs, work;
   if ((s = nshort.reserve(n)) || (s = tot.reserve(n)) || (s = curl.reserve(n)) || (s = curs.reserve(n)) ||
-      (s = work.reserve(n)))
+      (s = work.reserve(n)) || (s = sstart.reserve(nnz)) || (s = slen.reserve(nnz)))
     return bail(s);
   cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(nshort.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
-  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, cfg, p->plong.p, nshort.p);
+  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, cfg, p->plong.p, nshort.p,
+                                                     sstart.p, slen.p);
   k_partner_sizes<<<grid_for(n), 256, 0, st>>>(n, p->plong.p, nshort.p, tot.p);
   if ((s = scan_i64(n, tot.p, p->poff.p, st))) return bail(s);
   k_partner_cursors<<<grid_for(n), 256, 0, st>>>(n, p->poff.p, p->plong.p, curl.p, curs.p);
-  k_partner_fill<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, cfg, curl.p, curs.p, p->padj.p,
-                                                    work.p);
+  k_partner_fill<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, cfg, sstart.p, slen.p, curl.p,
+                                                    curs.p, p->pseg.p, work.p);
   // 3. task queues, heaviest first
   DevBuf<unsigned long long> ckey, wkey;
   DevBuf<int32_t> cval, wval;
@@ -594,11 +638,11 @@ int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long l
   if (g->nnz == 0) return GPM_OK;
   GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 4 * sizeof(int), st));
   if (rec)
-    k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->padj.p,
+    k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p,
                                                            p->plong.p, p->cta_tasks.p, p->n_cta, p->warp_tasks.p,
                                                            p->n_warp, p->counters.p, d_out, rec);
   else
-    k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->padj.p, p->plong.p,
+    k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p, p->plong.p,
                                                    p->cta_tasks.p, p->n_cta, p->warp_tasks.p, p->n_warp,
                                                    p->counters.p, d_out, nullptr);
   GPM_LAUNCH_CHECK();

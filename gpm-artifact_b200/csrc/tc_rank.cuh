@@ -17,14 +17,18 @@ struct RankGraph {
 };
 
 // Per-graph schedule of GPM_TC_BITMAP (device arrays):
-//   poff/padj   partner CSR: for owner x, the vertices whose lists are
-//               streamed against N(x); the first plong[x] are long lists
+//   poff/pseg   partner segments: for owner x, pseg[poff[x] .. poff[x+1])
+//               are [start, end) ranges of radj, each the part of one
+//               partner's list that lies inside [min N(x), max N(x)] (no
+//               key outside that range can be in N(x)); empty ranges are
+//               left out; the first plong[x] are long segments
 //   cta_tasks / warp_tasks  owners by size class, heaviest first
 struct RankPlan {
   int cta_min = 0, long_min = 0;
   int n_cta = 0, n_warp = 0;
   DevBuf<int64_t> poff;
-  DevBuf<int32_t> padj, plong;
+  DevBuf<longlong2> pseg;
+  DevBuf<int32_t> plong;
   DevBuf<int32_t> cta_tasks, warp_tasks;
   DevBuf<int> counters;
 };

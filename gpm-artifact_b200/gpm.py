@@ -285,7 +285,7 @@ class Sched:
     """Owning wrapper of the learned task scheduler (gpm_sched)."""
 
     # Parameters trained on logged task costs of R-MAT (scales 15-18) and
-    # Chung-Lu graphs; the training recipe is tests/test_sched_gpu.py's.
+    # Chung-Lu graphs; written by train_sched.py beside this file.
     PRETRAINED = os.path.join(HERE, "sched_tc.f32")
 
     def __init__(self, seed=1):
@@ -351,10 +351,13 @@ class Sched:
     def attach(self, g: "Graph"):
         check(lib.gpm_sched_attach(g.h, self.h))
 
+    _default = None  # the process default, kept alive while it is the default
+
     def set_default(self):
-        """Use this scheduler for every graph without an attached one (keep
-        the object alive meanwhile)."""
+        """Use this scheduler for every graph without an attached one."""
         check(lib.gpm_sched_set_default(self.h))
+        Sched._default = self
+        return self
 
     def assign(self, g: "Graph"):
         n = g.info().n

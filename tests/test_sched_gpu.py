@@ -79,3 +79,32 @@ def test_learned_schedule_counts_and_gain(trained):
     print(f"held-out R-MAT 18: warp-cycles heuristic {t_heur:.4g} learned {t_learn:.4g} best {t_best:.4g}")
     assert t_best <= t_learn
     assert t_learn <= t_heur, "the trained schedule should not cost more than the fixed heuristic"
+
+
+def test_scheduler_lifetime():
+    """A destroyed scheduler is never used: destroying the process default
+    clears it, and a graph whose attached scheduler was destroyed gets an
+    error instead of a launch."""
+    import torch
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    sp = torch.cuda.current_stream().cuda_stream
+    g = gpm.Graph.rmat(10, 8, seed=3).orient()
+    s = gpm.Sched(seed=5).set_default()
+    gpm.Sched._default = None
+    s.close()
+    with pytest.raises(gpm.GpmError, match="no trained scheduler"):
+        g.tc_async(gpm.TC_LEARNED, sp, out.data_ptr())
+    s2 = gpm.Sched(seed=6)
+    s2.attach(g)
+    lib, h = gpm.lib, s2.h
+    assert lib.gpm_sched_destroy(h) == 0
+    s2.h = None
+    with pytest.raises(gpm.GpmError, match="destroyed"):
+        g.tc_async(gpm.TC_LEARNED, sp, out.data_ptr())
+    assert lib.gpm_sched_set_default(h) != 0
+    assert lib.gpm_sched_destroy(h) != 0
+    s3 = gpm.Sched.pretrained()
+    s3.attach(g)
+    g.tc_async(gpm.TC_LEARNED, sp, out.data_ptr())
+    torch.cuda.synchronize()
+    assert int(out.item()) == g.tc(gpm.V_CENTRIC)
