@@ -184,8 +184,8 @@ __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restr
   f[3] = log2f(1.f + (float)mx);
   f[4] = log2f(1.f + (float)nlong);
   f[5] = log2f(1.f + (float)span);
-  f[6] = span <= (1ll << 17) ? 1.f : 0.f;
-  f[7] = span <= (1ll << 14) ? 1.f : 0.f;
+  f[6] = span <= 32ll * kRankCtaWords ? 1.f : 0.f;      // fits the CTA bitmap
+  f[7] = span <= 32ll * kRankCtaWords / 8 ? 1.f : 0.f;  // fits a warp's bitmap
 }
 
 __global__ void k_features(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
@@ -238,7 +238,7 @@ static int blocks(int64_t work) { return (int)std::max<int64_t>(1, std::min<int6
 
 // all owners of the heuristic plan, in one device list
 static int all_tasks(gpm_graph *g, DevBuf<int32_t> &tasks, int *ntasks, cudaStream_t st) {
-  GPM_TRY(rank_build_plan(g, 100, 32, st));
+  GPM_TRY(rank_build_plan(g, kRankCtaMin, kRankLongMin, st));
   RankPlan *p = g->rank;
   *ntasks = p->n_cta + p->n_warp;
   GPM_TRY(tasks.reserve(std::max(1, *ntasks)));
@@ -285,7 +285,7 @@ int tc_learned_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) 
                                                          h->pseg.p, s->w.p, cfg.p);
     GPM_LAUNCH_CHECK();
     RankPlan *p = nullptr;
-    GPM_TRY(rank_plan_new(g, 100, 32, cfg.p, st, &p));
+    GPM_TRY(rank_plan_new(g, kRankCtaMin, kRankLongMin, cfg.p, st, &p));
     g->learned = p;
   }
   return rank_plan_launch(g, g->learned, st, d_out, nullptr);
@@ -387,7 +387,7 @@ int gpm_sched_collect(gpm_sched *s, gpm_graph *g, int64_t *rows_added) {
   for (int c = 0; c < kOut; ++c) {
     GPM_CUDA(cudaMemsetAsync(cfg.p, c, g->n, st));
     RankPlan *p = nullptr;
-    GPM_TRY(rank_plan_new(g, 100, 32, cfg.p, st, &p));
+    GPM_TRY(rank_plan_new(g, kRankCtaMin, kRankLongMin, cfg.p, st, &p));
     int s1 = rank_plan_launch(g, p, st, cnt.p, nullptr);  // warm the caches
     if (s1 == GPM_OK) s1 = rank_plan_launch(g, p, st, cnt.p, rec.p);
     if (s1 == GPM_OK)

@@ -12,15 +12,19 @@
 //    owner task loads N(owner) once and streams the lists N(partner) of all
 //    its partners.  The streamed work is sum over edges of
 //    min(d(u), d(v)) instead of sum d(v) (2.3x less on R-MAT).
-// 3. Direct-mapped bitmap.  After the relabel nearly every owner list spans
-//    fewer than 2^17 ids, so membership is one shared-memory bit test (no
-//    hashing, no probe loops, no divergence).  Owners whose span is wider
-//    fall back to an open-addressing table.
+// 3. Clipped segments.  Only the part of N(partner) inside
+//    [min N(owner), max N(owner)] can meet N(owner); the plan stores that
+//    range of radj per edge (two binary searches at plan time), which drops
+//    another 30 % of the streamed keys on R-MAT and every range check.
+// 4. Direct-mapped membership.  After the relabel nearly every large owner
+//    list spans few ids, so membership is one shared-memory byte load (span
+//    within the byte map) or bit test (within the bitmap): no hashing, no
+//    probe loops, no divergence.  Wider owners use an open-addressing table.
 //
-// Long partner lists are streamed by a whole warp with 16-byte vector loads;
-// short ones by 8-lane groups.  Owners with more than `cta_min` keys are CTA
-// tasks, the rest warp tasks; both queues are sorted heaviest first and
-// drained by a persistent grid.
+// Long segments are streamed by a whole warp, one coalesced row of 32 keys
+// per step; short ones by 8-lane groups.  Owners with more than `cta_min`
+// keys are CTA tasks, the rest warp tasks; both queues are sorted heaviest
+// first and drained by a persistent grid.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -32,11 +36,9 @@
 namespace gpm {
 
 constexpr int kRWarps = 8;
-constexpr int kCtaWords = 4096;        // 16 KB: bitmap of 2^17 bits or 4096 hash slots
-constexpr int kWarpWords = 512;        // 2 KB per warp: 2^14 bits or 512 hash slots
-constexpr int kCtaHashChunk = 2048;    // keys per hash chunk (load <= 0.5)
-constexpr int kWarpHashChunk = 256;
-static_assert(kWarpWords * kRWarps == kCtaWords, "warp regions tile the CTA region");
+constexpr int kCtaWords = kRankCtaWords;
+constexpr int kWarpWords = kCtaWords / kRWarps;
+static_assert(kWarpWords >= 64 && kWarpWords * kRWarps == kCtaWords, "warp regions tile the CTA region");
 constexpr size_t kRankSmem = kCtaWords * 4;
 
 static int grid_for(int64_t work, int block = 256) {
@@ -47,8 +49,13 @@ static int grid_for(int64_t work, int block = 256) {
 
 // ------------------------------------------------------------ membership
 // Every key handed to a table lies in [min N(owner), max N(owner)]: the plan
-// clipped the partner segments to that range, so the bitmap needs no range
+// clipped the partner segments to that range, so the maps need no range
 // check.
+struct ByteTable {
+  const uint8_t *bm;
+  int32_t base;
+  __device__ __forceinline__ unsigned hit(int32_t w) const { return bm[w - base]; }
+};
 struct BitTable {
   const uint32_t *bm;
   int32_t base;
@@ -125,57 +132,29 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
 __device__ __forceinline__ int ceil_log2i(int x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
 
 // ------------------------------------------------------------ tasks
-__device__ unsigned long long rank_cta_task(int32_t x, const int64_t *__restrict__ roff,
-                                            const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                                            const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
-                                            uint32_t *words) {
-  const int tid = threadIdx.x, nthr = blockDim.x, wid = tid >> 5, nw = nthr >> 5;
-  const unsigned lane = tid & 31;
-  const int64_t s0 = roff[x];
-  const int d = (int)(roff[x + 1] - s0);
-  const int64_t p0 = poff[x], p1 = poff[x + 1];
-  const int nl = plong[x];
-  const int32_t kmin = radj[s0], kmax = radj[s0 + d - 1];
-  const int64_t span = (int64_t)kmax - kmin + 1;
-  unsigned long long c = 0;
-  if (span <= (int64_t)kCtaWords * 32) {
-    const int nwords = (int)((span + 31) >> 5);
-    for (int i = tid; i < nwords; i += nthr) words[i] = 0u;
+template <bool CTA>
+__device__ __forceinline__ void group_sync() {
+  if (CTA)
     __syncthreads();
-    for (int i = tid; i < d; i += nthr) {
-      uint32_t o = (uint32_t)(radj[s0 + i] - kmin);
-      atomicOr(&words[o >> 5], 1u << (o & 31));
-    }
-    __syncthreads();
-    BitTable t{words, kmin};
-    c = scan_segments(radj, pseg, p0, p1, nl, t, wid, nw, lane);
-  } else {
-    int32_t *tab = reinterpret_cast<int32_t *>(words);
-    for (int t0 = 0; t0 < d; t0 += kCtaHashChunk) {
-      const int tk = min(kCtaHashChunk, d - t0);
-      const int logcap = max(5, ceil_log2i(2 * tk));
-      const uint32_t mask = (1u << logcap) - 1u;
-      __syncthreads();
-      for (int i = tid; i < (1 << logcap); i += nthr) tab[i] = -1;
-      __syncthreads();
-      for (int i = tid; i < tk; i += nthr) {
-        int32_t key = radj[s0 + t0 + i];
-        uint32_t h = ((uint32_t)key * 2654435769u) >> (32 - logcap);
-        while (atomicCAS(&tab[h], -1, key) != -1) h = (h + 1) & mask;
-      }
-      __syncthreads();
-      HashTable t{tab, logcap};
-      c += scan_segments(radj, pseg, p0, p1, nl, t, wid, nw, lane);
-    }
-  }
-  __syncthreads();
-  return c;
+  else
+    __syncwarp();
 }
 
-__device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restrict__ roff,
-                                             const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                                             const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
-                                             uint32_t *words) {
+// One owner task: the membership structure of N(x) in `words` (nwords
+// 32-bit words of shared memory), built by the group's threads (the CTA, or
+// one warp), then the owner's segments streamed against it.  By the span S of
+// N(x): S <= 4 * nwords -> byte map; S <= 32 * nwords -> bitmap; else
+// open-addressing tables of the largest power-of-two size that fits, built
+// over chunks of at most half that many keys.
+template <bool CTA>
+__device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_t *__restrict__ roff,
+                                                         const int32_t *__restrict__ radj,
+                                                         const int64_t *__restrict__ poff,
+                                                         const longlong2 *__restrict__ pseg,
+                                                         const int32_t *__restrict__ plong, uint32_t *words,
+                                                         int nwords) {
+  const int tid = CTA ? (int)threadIdx.x : (int)lane_id(), nthr = CTA ? (int)blockDim.x : 32;
+  const int wid = CTA ? tid >> 5 : 0, nw = CTA ? nthr >> 5 : 1;
   const unsigned lane = lane_id();
   const int64_t s0 = roff[x];
   const int d = (int)(roff[x + 1] - s0);
@@ -184,37 +163,44 @@ __device__ unsigned long long rank_warp_task(int32_t x, const int64_t *__restric
   const int32_t kmin = radj[s0], kmax = radj[s0 + d - 1];
   const int64_t span = (int64_t)kmax - kmin + 1;
   unsigned long long c = 0;
-  if (span <= (int64_t)kWarpWords * 32) {
-    const int nwords = (int)((span + 31) >> 5);
-    for (int i = lane; i < nwords; i += 32) words[i] = 0u;
-    __syncwarp();
-    for (int i = lane; i < d; i += 32) {
+  if (span <= (int64_t)nwords * 4) {
+    const int nclear = (int)((span + 3) >> 2);
+    for (int i = tid; i < nclear; i += nthr) words[i] = 0u;
+    group_sync<CTA>();
+    uint8_t *bytes = reinterpret_cast<uint8_t *>(words);
+    for (int i = tid; i < d; i += nthr) bytes[radj[s0 + i] - kmin] = 1;
+    group_sync<CTA>();
+    c = scan_segments(radj, pseg, p0, p1, nl, ByteTable{bytes, kmin}, wid, nw, lane);
+  } else if (span <= (int64_t)nwords * 32) {
+    const int nclear = (int)((span + 31) >> 5);
+    for (int i = tid; i < nclear; i += nthr) words[i] = 0u;
+    group_sync<CTA>();
+    for (int i = tid; i < d; i += nthr) {
       uint32_t o = (uint32_t)(radj[s0 + i] - kmin);
       atomicOr(&words[o >> 5], 1u << (o & 31));
     }
-    __syncwarp();
-    BitTable t{words, kmin};
-    c = scan_segments(radj, pseg, p0, p1, nl, t, 0, 1, lane);
+    group_sync<CTA>();
+    c = scan_segments(radj, pseg, p0, p1, nl, BitTable{words, kmin}, wid, nw, lane);
   } else {
     int32_t *tab = reinterpret_cast<int32_t *>(words);
-    for (int t0 = 0; t0 < d; t0 += kWarpHashChunk) {
-      const int tk = min(kWarpHashChunk, d - t0);
-      const int logcap = max(5, ceil_log2i(2 * tk));
-      const uint32_t mask = (1u << logcap) - 1u;
-      __syncwarp();
-      for (int i = lane; i < (1 << logcap); i += 32) tab[i] = -1;
-      __syncwarp();
-      for (int i = lane; i < tk; i += 32) {
+    const int logcap = 31 - __clz(nwords);
+    const int chunk = 1 << (logcap - 1);
+    const uint32_t mask = (1u << logcap) - 1u;
+    for (int t0 = 0; t0 < d; t0 += chunk) {
+      const int tk = min(chunk, d - t0);
+      group_sync<CTA>();
+      for (int i = tid; i < (1 << logcap); i += nthr) tab[i] = -1;
+      group_sync<CTA>();
+      for (int i = tid; i < tk; i += nthr) {
         int32_t key = radj[s0 + t0 + i];
         uint32_t h = ((uint32_t)key * 2654435769u) >> (32 - logcap);
         while (atomicCAS(&tab[h], -1, key) != -1) h = (h + 1) & mask;
       }
-      __syncwarp();
-      HashTable t{tab, logcap};
-      c += scan_segments(radj, pseg, p0, p1, nl, t, 0, 1, lane);
+      group_sync<CTA>();
+      c += scan_segments(radj, pseg, p0, p1, nl, HashTable{tab, logcap}, wid, nw, lane);
     }
   }
-  __syncwarp();
+  group_sync<CTA>();
   return c;
 }
 
@@ -244,7 +230,7 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     if (t >= n_cta) break;
     const int32_t x = cta_tasks[t];
     long long t0 = REC ? clock64() : 0;
-    c += rank_cta_task(x, roff, radj, poff, pseg, plong, rsm);
+    c += owner_task<true>(x, roff, radj, poff, pseg, plong, rsm, kCtaWords);
     if (REC && threadIdx.x == 0) rec[x] = (unsigned long long)(clock64() - t0) * (blockDim.x >> 5);
   }
   const int wid = threadIdx.x >> 5;
@@ -257,7 +243,7 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     if (t >= n_warp) break;
     const int32_t x = warp_tasks[t];
     long long t0 = REC ? clock64() : 0;
-    c += rank_warp_task(x, roff, radj, poff, pseg, plong, region);
+    c += owner_task<false>(x, roff, radj, poff, pseg, plong, region, kWarpWords);
     if (REC && lane == 0) rec[x] = (unsigned long long)(clock64() - t0);
   }
   c = warp_sum(c);
@@ -651,9 +637,9 @@ int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long l
 
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
   if (g->nnz == 0) return cudaMemsetAsync(d_out, 0, 8, st) == cudaSuccess ? GPM_OK : GPM_ECUDA;
-  // reference-style fixed thresholds: owners with > 100 keys go to a CTA,
-  // lists of >= 32 ids are streamed by a whole warp
-  GPM_TRY(rank_build_plan(g, 100, 32, st));
+  // fixed schedule: owners with > kRankCtaMin keys go to a CTA, segments of
+  // >= kRankLongMin keys are streamed by a whole warp
+  GPM_TRY(rank_build_plan(g, kRankCtaMin, kRankLongMin, st));
   return rank_plan_launch(g, g->rank, st, d_out, nullptr);
 }
 

@@ -5,6 +5,25 @@
 
 namespace gpm {
 
+#ifndef GPM_RANK_CTA_WORDS
+// 24 KB of shared memory per CTA of the count kernel (8 CTAs = 192 KB of an
+// SM's 228 KB): a byte map of 24,576 ids, a bitmap of 196,608 ids or a
+// 4096-slot hash table; a warp task gets an eighth (3,072 ids / 24,576 ids /
+// 512 slots)
+#define GPM_RANK_CTA_WORDS 6144
+#endif
+constexpr int kRankCtaWords = GPM_RANK_CTA_WORDS;
+#ifndef GPM_RANK_CTA_MIN
+// fixed schedule: owners with more keys than this are CTA tasks (R-MAT 22:
+// 7.65 ms at 50 against 8.0 ms at the reference's USE_CTA = 100 and 7.67 ms
+// at 70; smaller owners rarely fit a warp's bitmap and hash instead)
+#define GPM_RANK_CTA_MIN 50
+#endif
+constexpr int kRankCtaMin = GPM_RANK_CTA_MIN;
+// fixed schedule: partner segments of at least this many keys are streamed
+// by a whole warp, shorter ones by 8-lane groups
+constexpr int kRankLongMin = 32;
+
 // The stored graph renumbered by (in + out degree, id) rank, lists sorted.
 // upward == 1 when every stored edge points to a larger rank, which holds
 // for a degree-oriented DAG (orientation rule of graph.h:128-129); then
