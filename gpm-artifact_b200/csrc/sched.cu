@@ -5,10 +5,11 @@
 // fallback and as the yardstick of the learned schedule's regret).
 //
 // Decision per owner task of GPM_TC_BITMAP (tc_rank.cu): one of 6
-// configurations = queue (warp | CTA) x long-list threshold (8 | 32 | 128).
+// configurations = queue (warp | CTA) x long-segment threshold (16 | 64 | 256).
 // Counts do not depend on the choice; only time does.
 //
-// Data: the engine logs, for every owner, its cost in warp-cycles under each
+// Data: the engine logs, for every owner, its cost in active warp-cycles (the
+// cycles each of its warps spent on it, barrier waits excluded) under each
 // configuration (instrumented kernel k_tc_rank_t<true>) together with 8
 // features of the task (list and partner sizes, key span) -- the
 // intersection-size trace of the owner.
@@ -208,17 +209,23 @@ __global__ void k_gather_costs(const int32_t *__restrict__ tasks, int ntasks, co
     Y[t * kOut + cfg] = log2f(1.f + (float)rec[tasks[t]]);
 }
 
-// Fused scheduler: features + MLP inference + argmin -> cfg[owner].
+// Fused scheduler: features + MLP inference + argmin -> cfg[owner].  For a
+// task whose cheapest configuration is a warp one, its predicted cost and
+// its cheapest CTA configuration go to warp_cost[t] / cta_alt[t] (0 / -
+// otherwise); every task's predicted cost is summed into *total.
 __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ tasks, int ntasks,
                                                 const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
                                                 const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
-                                                const float *__restrict__ w, uint8_t *__restrict__ cfg) {
+                                                const float *__restrict__ w, uint8_t *__restrict__ cfg,
+                                                float *__restrict__ warp_cost, uint8_t *__restrict__ cta_alt,
+                                                double *__restrict__ total) {
   __shared__ float sw[kParams];
   for (int i = threadIdx.x; i < kParams; i += blockDim.x) sw[i] = w[i];
   __syncthreads();
   const unsigned lane = lane_id();
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  double sum = 0;
   for (int64_t t = warp; t < ntasks; t += nw) {
     float f[kIn];
     const int32_t x = tasks[t];
@@ -226,12 +233,32 @@ __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ task
     if (lane == 0) {
       float h1[kH], h2[kH], y[kOut];
       mlp_forward(sw, f, h1, h2, y);
-      int best = 0;
+      int best = 0, cta = kOut / 2;
       for (int k = 1; k < kOut; ++k)
         if (y[k] < y[best]) best = k;
+      for (int k = kOut / 2 + 1; k < kOut; ++k)
+        if (y[k] < y[cta]) cta = k;
+      const float cost = exp2f(y[best]) - 1.f;
       cfg[x] = (uint8_t)best;
+      warp_cost[t] = best < kOut / 2 ? cost : 0.f;
+      cta_alt[t] = (uint8_t)cta;
+      sum += cost;
     }
   }
+  if (lane == 0 && sum > 0) atomicAdd(total, sum);
+}
+
+// Makespan rail.  The CTA queue drains first and the warp queue last, so a
+// warp task predicted to cost more than kRail x (total / warp slots) would
+// run on after every other warp is done; it takes its cheapest CTA
+// configuration instead, spreading it over a CTA's 8 warps.
+constexpr float kRail = 0.5f;
+__global__ void k_rail(const int32_t *__restrict__ tasks, int ntasks, const float *__restrict__ warp_cost,
+                       const uint8_t *__restrict__ cta_alt, const double *__restrict__ total, double slots,
+                       uint8_t *__restrict__ cfg) {
+  const float bound = (float)(kRail * *total / slots);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntasks; t += (int64_t)gridDim.x * blockDim.x)
+    if (warp_cost[t] > bound) cfg[tasks[t]] = cta_alt[t];
 }
 
 static int blocks(int64_t work) { return (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, num_sms() * 8)); }
@@ -247,6 +274,28 @@ static int all_tasks(gpm_graph *g, DevBuf<int32_t> &tasks, int *ntasks, cudaStre
   if (p->n_warp)
     GPM_CUDA(cudaMemcpyAsync(tasks.p + p->n_cta, p->warp_tasks.p, sizeof(int32_t) * p->n_warp,
                              cudaMemcpyDeviceToDevice, st));
+  return GPM_OK;
+}
+
+// Configuration of every task of the fixed plan under scheduler s into cfg
+// (device, one byte per vertex; entries of non-tasks are left as they are).
+static int assign_configs(gpm_graph *g, gpm_sched *s, const int32_t *tasks, int nt, uint8_t *cfg, cudaStream_t st) {
+  if (nt <= 0) return GPM_OK;
+  DevBuf<float> warp_cost;
+  DevBuf<uint8_t> cta_alt;
+  DevBuf<double> total;
+  GPM_TRY(warp_cost.reserve(nt));
+  GPM_TRY(cta_alt.reserve(nt));
+  GPM_TRY(total.reserve(1));
+  GPM_CUDA(cudaMemsetAsync(total.p, 0, sizeof(double), st));
+  RankPlan *h = g->rank;
+  k_assign<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p, h->pseg.p,
+                                                     s->w.p, cfg, warp_cost.p, cta_alt.p, total.p);
+  GPM_LAUNCH_CHECK();
+  // warp slots of the count kernel: 8 CTAs of 8 warps per SM
+  k_rail<<<blocks(nt), 256, 0, st>>>(tasks, nt, warp_cost.p, cta_alt.p, total.p, 64.0 * num_sms(), cfg);
+  GPM_LAUNCH_CHECK();
+  GPM_CUDA(cudaStreamSynchronize(st));
   return GPM_OK;
 }
 
@@ -279,11 +328,7 @@ int tc_learned_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) 
     GPM_TRY(cfg.reserve(g->n));
     // owners that are not tasks keep the heuristic's class (unused)
     GPM_CUDA(cudaMemsetAsync(cfg.p, 1, g->n, st));
-    RankPlan *h = g->rank;
-    if (nt > 0)
-      k_assign<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p,
-                                                         h->pseg.p, s->w.p, cfg.p);
-    GPM_LAUNCH_CHECK();
+    GPM_TRY(assign_configs(g, s, tasks.p, nt, cfg.p, st));
     RankPlan *p = nullptr;
     GPM_TRY(rank_plan_new(g, kRankCtaMin, kRankLongMin, cfg.p, st, &p));
     g->learned = p;
@@ -353,7 +398,7 @@ int gpm_sched_set_params(gpm_sched *s, const float *params) {
 }
 
 // Logs every owner task of g under each of the 6 configurations and appends
-// (features, log2 warp-cycles) rows to the dataset.
+// (features, log2 active warp-cycles) rows to the dataset.
 int gpm_sched_collect(gpm_sched *s, gpm_graph *g, int64_t *rows_added) {
   if (!s || !g) return fail(GPM_EINVAL, "NULL argument");
   cudaStream_t st = 0;
@@ -389,6 +434,8 @@ int gpm_sched_collect(gpm_sched *s, gpm_graph *g, int64_t *rows_added) {
     RankPlan *p = nullptr;
     GPM_TRY(rank_plan_new(g, kRankCtaMin, kRankLongMin, cfg.p, st, &p));
     int s1 = rank_plan_launch(g, p, st, cnt.p, nullptr);  // warm the caches
+    if (s1 == GPM_OK && cudaMemsetAsync(rec.p, 0, sizeof(unsigned long long) * g->n, st) != cudaSuccess)
+      s1 = fail(GPM_ECUDA, "memset");
     if (s1 == GPM_OK) s1 = rank_plan_launch(g, p, st, cnt.p, rec.p);
     if (s1 == GPM_OK)
       k_gather_costs<<<blocks(nt), 256, 0, st>>>(tasks.p, nt, rec.p, c, s->Y.p + s->rows * kOut);
@@ -491,11 +538,7 @@ int gpm_sched_assign(gpm_sched *s, gpm_graph *g, uint8_t *cfg) {
   DevBuf<uint8_t> d;
   GPM_TRY(d.reserve(g->n));
   GPM_CUDA(cudaMemset(d.p, 255, g->n));
-  RankPlan *h = g->rank;
-  if (nt > 0)
-    k_assign<<<blocks((int64_t)nt * 32), 256>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p, h->pseg.p,
-                                               s->w.p, d.p);
-  GPM_LAUNCH_CHECK();
+  GPM_TRY(assign_configs(g, s, tasks.p, nt, d.p, 0));
   GPM_CUDA(cudaMemcpy(cfg, d.p, g->n, cudaMemcpyDeviceToHost));
   return GPM_OK;
 }

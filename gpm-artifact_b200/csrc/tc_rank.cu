@@ -1,7 +1,7 @@
 // tc_rank.cu -- the B200 triangle-count path (variant GPM_TC_BITMAP).
 //
 // Same sum as every TCSolver variant, T = sum over stored u->v of
-// |N(u) & N(v)|, reorganised three ways:
+// |N(u) & N(v)|, reorganised four ways:
 //
 // 1. Rank relabel.  Vertices are renumbered by (in+out degree, id), the
 //    order the degree orientation (graph.h:128-129) is built on, so a DAG
@@ -21,10 +21,10 @@
 //    within the byte map) or bit test (within the bitmap): no hashing, no
 //    probe loops, no divergence.  Wider owners use an open-addressing table.
 //
-// Long segments are streamed by a whole warp, one coalesced row of 32 keys
-// per step; short ones by 8-lane groups.  Owners with more than `cta_min`
-// keys are CTA tasks, the rest warp tasks; both queues are sorted heaviest
-// first and drained by a persistent grid.
+// Long segments are streamed by half-warps, one coalesced row of 16 keys per
+// step; short ones by 8-lane groups.  Owners with more than `cta_min` keys
+// are CTA tasks, the rest warp tasks; both queues are sorted heaviest first
+// and drained by a persistent grid.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -79,30 +79,13 @@ struct HashTable {
   }
 };
 
-// One segment of radj streamed by the whole warp, one key per lane per step
-// (each step one coalesced 128-byte row).  The loop bounds are the same for
-// every lane: full 128-key blocks with four loads in flight per lane, then at
-// most four single steps, so a segment of L keys takes ceil(L / 32) steps.
-template <class T>
-__device__ __forceinline__ unsigned warp_segment(const int32_t *__restrict__ radj, longlong2 sg, const T &t,
-                                                 unsigned lane) {
-  const int32_t *__restrict__ q = radj + sg.x;
-  const int len = (int)(sg.y - sg.x);
-  const int full = len & ~127;
-  unsigned c = 0;
-  int i = (int)lane;
-  for (; i < full; i += 128) {
-    const int32_t a = __ldg(q + i), b = __ldg(q + i + 32), d = __ldg(q + i + 64), e = __ldg(q + i + 96);
-    c += t.hit(a) + t.hit(b) + t.hit(d) + t.hit(e);
-  }
-  for (; i < len; i += 32) c += t.hit(__ldg(q + i));
-  return c;
-}
-
-// Segments [p0, p1) of one owner: the first nlong are long (a whole warp
-// each, the next descriptor loaded while the current one streams), the rest
-// short (8-lane groups).  `wid`/`nw` spread segments over the warps of the
-// executing group (1 warp for warp tasks, the CTA's warps for CTA tasks).
+// Segments [p0, p1) of one owner.  The first nlong are long: each half-warp
+// streams one, 16 keys per step (each step one coalesced 64-byte row), so
+// the per-segment work of a warp is shared by two segments; the rest are
+// short: 8-lane groups, four segments per warp.  `wid`/`nw` spread segments
+// over the warps of the executing group (1 warp for warp tasks, the CTA's
+// warps for CTA tasks).  R-MAT 22: half-warps 7.0 ms against 7.6 ms for
+// whole-warp streaming of the same segments.
 template <class T>
 __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__restrict__ radj,
                                                             const longlong2 *__restrict__ pseg, int64_t p0,
@@ -110,14 +93,16 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
                                                             unsigned lane) {
   unsigned long long c = 0;
   const int64_t pl = p0 + nlong;
-  int64_t j = p0 + wid;
-  if (j < pl) {
-    longlong2 nx = pseg[j];
-    for (; j < pl; j += nw) {
-      const longlong2 sg = nx;
-      if (j + nw < pl) nx = pseg[j + nw];
-      c += warp_segment(radj, sg, t, lane);
-    }
+  const unsigned half = lane >> 4, hl = lane & 15;
+  int64_t j;
+  for (j = p0 + wid * 2 + half; j < pl; j += nw * 2) {
+    const longlong2 sg = pseg[j];
+    const int32_t *__restrict__ q = radj + sg.x;
+    const int len = (int)(sg.y - sg.x);
+    unsigned cs = 0;
+#pragma unroll 4
+    for (int i = (int)hl; i < len; i += 16) cs += t.hit(__ldg(q + i));
+    c += cs;
   }
   const unsigned grp = lane >> 3, gl = lane & 7;
   for (j = pl + wid * 4 + grp; j < p1; j += nw * 4) {
@@ -128,8 +113,6 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
   }
   return c;
 }
-
-__device__ __forceinline__ int ceil_log2i(int x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
 
 // ------------------------------------------------------------ tasks
 template <bool CTA>
@@ -145,14 +128,17 @@ __device__ __forceinline__ void group_sync() {
 // one warp), then the owner's segments streamed against it.  By the span S of
 // N(x): S <= 4 * nwords -> byte map; S <= 32 * nwords -> bitmap; else
 // open-addressing tables of the largest power-of-two size that fits, built
-// over chunks of at most half that many keys.
-template <bool CTA>
+// over chunks of at most half that many keys.  REC: each warp adds the
+// cycles it was busy on the task (to just before the closing barrier) to
+// *rec, so a task's logged cost is its active warp-cycles.
+template <bool CTA, bool REC>
 __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_t *__restrict__ roff,
                                                          const int32_t *__restrict__ radj,
                                                          const int64_t *__restrict__ poff,
                                                          const longlong2 *__restrict__ pseg,
                                                          const int32_t *__restrict__ plong, uint32_t *words,
-                                                         int nwords) {
+                                                         int nwords, unsigned long long *rec) {
+  const long long t0 = REC ? clock64() : 0;
   const int tid = CTA ? (int)threadIdx.x : (int)lane_id(), nthr = CTA ? (int)blockDim.x : 32;
   const int wid = CTA ? tid >> 5 : 0, nw = CTA ? nthr >> 5 : 1;
   const unsigned lane = lane_id();
@@ -200,6 +186,7 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
       c += scan_segments(radj, pseg, p0, p1, nl, HashTable{tab, logcap}, wid, nw, lane);
     }
   }
+  if (REC && lane == 0) atomicAdd(rec, (unsigned long long)(clock64() - t0));
   group_sync<CTA>();
   return c;
 }
@@ -210,8 +197,9 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
 #define GPM_TC_RANK_MIN_BLOCKS 8
 #endif
 // REC = true is the instrumented build the learned scheduler trains on: it
-// logs each task's cost in warp-cycles (SM clock cycles x warps the task
-// occupied) into rec[owner].
+// adds each task's active warp-cycles (per warp, the SM clock cycles it spent
+// on the task outside the closing barrier) into rec[owner], which the caller
+// zeroes first.
 template <bool REC>
 __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     k_tc_rank_t(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
@@ -229,9 +217,7 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     __syncthreads();
     if (t >= n_cta) break;
     const int32_t x = cta_tasks[t];
-    long long t0 = REC ? clock64() : 0;
-    c += owner_task<true>(x, roff, radj, poff, pseg, plong, rsm, kCtaWords);
-    if (REC && threadIdx.x == 0) rec[x] = (unsigned long long)(clock64() - t0) * (blockDim.x >> 5);
+    c += owner_task<true, REC>(x, roff, radj, poff, pseg, plong, rsm, kCtaWords, REC ? rec + x : nullptr);
   }
   const int wid = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31;
@@ -242,9 +228,7 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= n_warp) break;
     const int32_t x = warp_tasks[t];
-    long long t0 = REC ? clock64() : 0;
-    c += owner_task<false>(x, roff, radj, poff, pseg, plong, region, kWarpWords);
-    if (REC && lane == 0) rec[x] = (unsigned long long)(clock64() - t0);
+    c += owner_task<false, REC>(x, roff, radj, poff, pseg, plong, region, kWarpWords, REC ? rec + x : nullptr);
   }
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(out, c);
@@ -321,8 +305,8 @@ __global__ void k_rank_up_copy(int64_t n, const int32_t *__restrict__ order, con
 }
 
 // Per-owner task configuration (learned scheduler): queue = cfg / 3
-// (0 warp, 1 CTA), long-list threshold = kCfgLong[cfg % 3].
-__device__ __constant__ int kCfgLong[3] = {8, 32, 128};
+// (0 warp, 1 CTA), long-segment threshold = kCfgLong[cfg % 3].
+__device__ __constant__ int kCfgLong[3] = {16, 64, 256};
 __device__ __forceinline__ int owner_long_min(const uint8_t *cfg, int32_t owner, int long_min) {
   return cfg ? kCfgLong[cfg[owner] % 3] : long_min;
 }

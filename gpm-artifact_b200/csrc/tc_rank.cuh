@@ -21,8 +21,9 @@ constexpr int kRankCtaWords = GPM_RANK_CTA_WORDS;
 #endif
 constexpr int kRankCtaMin = GPM_RANK_CTA_MIN;
 // fixed schedule: partner segments of at least this many keys are streamed
-// by a whole warp, shorter ones by 8-lane groups
-constexpr int kRankLongMin = 32;
+// by a half-warp, shorter ones by 8-lane groups (R-MAT 20: 1.35 ms at 64,
+// 1.38 ms at 32)
+constexpr int kRankLongMin = 64;
 
 // The stored graph renumbered by (in + out degree, id) rank, lists sorted.
 // upward == 1 when every stored edge points to a larger rank, which holds
@@ -59,10 +60,11 @@ int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid = nullpt
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st);
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out);
 // An uncached plan; cfg (device, one byte per vertex, may be nullptr) gives
-// each owner its queue (cfg / 3: 0 warp, 1 CTA) and long-list threshold
-// ({8, 32, 128}[cfg % 3]) instead of the fixed thresholds.
+// each owner its queue (cfg / 3: 0 warp, 1 CTA) and long-segment threshold
+// ({16, 64, 256}[cfg % 3]) instead of the fixed thresholds.
 int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, cudaStream_t st, RankPlan **out);
-// rec != nullptr: instrumented run logging each owner's cost (warp-cycles) to rec[owner]
+// rec != nullptr: instrumented run adding each owner's cost (active warp-cycles)
+// to rec[owner]; rec must be zeroed first
 int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long long *d_out,
                      unsigned long long *rec);
 

@@ -209,9 +209,12 @@ int gpm_pattern(gpm_graph *g, const char *name, int family, uint64_t *counters,
  * thresholds USE_CTA / USE_WARP of src/gpu_kernels/tuning_schedules.cuh:196-197,
  * which remain the default schedule and the yardstick of its regret) --------
  * Each owner task of GPM_TC_BITMAP gets one of 6 configurations:
- * queue (cfg / 3: 0 warp, 1 CTA) x long-list threshold ({8, 32, 128}[cfg % 3]).
- * A 3-layer FP32 MLP (8 -> 32 -> 32 -> 6) predicts log2 warp-cycles of each
- * configuration from 8 task features; counts never depend on the choice. */
+ * queue (cfg / 3: 0 warp, 1 CTA) x long-segment threshold ({16, 64, 256}[cfg % 3]).
+ * A 3-layer FP32 MLP (8 -> 32 -> 32 -> 6) predicts log2 active warp-cycles of
+ * each configuration from 8 task features; a task takes its cheapest one,
+ * except that a warp-queue task predicted to cost more than half a warp
+ * slot's share of the total takes its cheapest CTA configuration.  Counts
+ * never depend on the choice. */
 int gpm_sched_create(uint64_t seed, gpm_sched **out);
 int gpm_sched_destroy(gpm_sched *s);
 int gpm_sched_param_count(void);
@@ -227,10 +230,12 @@ int gpm_sched_grad(gpm_sched *s, int64_t N, const float *X, const float *T, floa
 int gpm_sched_predict(gpm_sched *s, int64_t N, const float *X, float *Y);
 /* Full-batch Adam steps on the collected dataset, trained on the device. */
 int gpm_sched_train(gpm_sched *s, int steps, float lr, double *final_loss);
-/* GPM_TC_LEARNED on g uses s from now on (s must outlive g's use of it). */
+/* GPM_TC_LEARNED on g uses s from now on; a destroyed scheduler is detected
+ * (GPM_EINVAL) instead of used. */
 int gpm_sched_attach(gpm_graph *g, gpm_sched *s);
 /* Scheduler used by GPM_TC_LEARNED on graphs without an attached one,
- * including the temporary graph of gpm_tc_host_csr (NULL clears it). */
+ * including the temporary graph of gpm_tc_host_csr (NULL clears it;
+ * destroying the default clears it too). */
 int gpm_sched_set_default(gpm_sched *s);
 /* The configuration the scheduler gives each vertex's task (255: no task). */
 int gpm_sched_assign(gpm_sched *s, gpm_graph *g, uint8_t *cfg);

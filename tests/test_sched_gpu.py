@@ -28,7 +28,7 @@ def test_device_gradient_matches_cpu_reference():
     assert np.allclose(s.predict(X), y, rtol=1e-4, atol=1e-4)
 
 
-HEUR = lambda X: np.where(np.exp2(X[:, 0]) - 1 > 50, 4, 1)  # the fixed schedule: CTA if d > 50, long threshold 32
+HEUR = lambda X: np.where(np.exp2(X[:, 0]) - 1 > 50, 4, 1)  # the fixed schedule: CTA if d > 50, long threshold 64
 
 
 def totals(X, Y, choice):
