@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (22 is the headline workload)")
-    ap.add_argument("--variant", default="learned",
+    ap.add_argument("--variant", default="auto",
                     choices=["auto", "bitmap", "hash", "bsearch", "merge", "learned"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -203,6 +203,11 @@ def main():
     n, m_und = inf.n, inf.nnz
     wedge, pair = g.work()
     bytes_alg = 4 * (n + 1) + 4 * m_und + 4 * wedge
+    # what this kernel streams: the clipped segments (4 B a key, a 16-byte
+    # descriptor each) and every owner list once, plus per owner 36 B of
+    # offsets and counts
+    nseg, seg_keys, owner_keys, ntasks = g.plan_stats()
+    bytes_kernel = 4 * seg_keys + 16 * nseg + 4 * owner_keys + 36 * ntasks
     variants = {"auto": gpm.TC_AUTO, "bitmap": gpm.TC_BITMAP, "hash": gpm.TC_HASH, "bsearch": gpm.TC_BSEARCH,
                 "merge": gpm.TC_MERGE, "learned": gpm.TC_LEARNED}
     variant = variants[args.variant]
@@ -244,8 +249,8 @@ def main():
 
     # ---- the other schedules on the same graph (outside the timed region)
     others = {}
-    for name in ("bitmap", "hash"):
-        if name == args.variant:
+    for name in ("bitmap", "learned", "hash"):
+        if name == args.variant or (name == "bitmap" and args.variant == "auto"):
             continue
         v = variants[name]
         g.tc_async(v, sp, out.data_ptr())
@@ -312,7 +317,15 @@ def main():
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes": bytes_alg, "kernel_ms": avg_kernel_ms},
+                         "traffic": traffic, "algorithmic_bytes": bytes_alg, "kernel_ms": avg_kernel_ms,
+                         # B_TC counts the vertex-iterator's reads (every wedge list in
+                         # full); this kernel streams only the clipped smaller side:
+                         "kernel_bytes": bytes_kernel,
+                         "kernel_bytes_gbs": bytes_kernel / (avg_kernel_ms / 1e3) / 1e9,
+                         "kernel_bytes_frac": bytes_kernel / (avg_kernel_ms / 1e3) / 1e9 / hbm,
+                         "dram_gbs": traffic / (avg_kernel_ms / 1e3) / 1e9 if traffic else None,
+                         "plan": {"segments": nseg, "segment_keys": seg_keys, "owner_keys": owner_keys,
+                                  "owner_tasks": ntasks}},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             # one count kernel per step (k_tc_rank, or k_tc_hash / k_tc_bsearch / k_tc_merge)

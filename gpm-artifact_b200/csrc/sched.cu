@@ -209,7 +209,8 @@ __global__ void k_gather_costs(const int32_t *__restrict__ tasks, int ntasks, co
     Y[t * kOut + cfg] = log2f(1.f + (float)rec[tasks[t]]);
 }
 
-// Fused scheduler: features + MLP inference + argmin -> cfg[owner].  For a
+// Fused scheduler: features + MLP inference + argmin -> cfg[owner] (over the
+// CTA configurations only for owners with more than kRankCtaMin keys).  For a
 // task whose cheapest configuration is a warp one, its predicted cost and
 // its cheapest CTA configuration go to warp_cost[t] / cta_alt[t] (0 / -
 // otherwise); every task's predicted cost is summed into *total.
@@ -233,11 +234,16 @@ __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ task
     if (lane == 0) {
       float h1[kH], h2[kH], y[kOut];
       mlp_forward(sw, f, h1, h2, y);
-      int best = 0, cta = kOut / 2;
-      for (int k = 1; k < kOut; ++k)
-        if (y[k] < y[best]) best = k;
+      // owners above the fixed CTA threshold stay CTA tasks (only their
+      // segment threshold is learned): demoting a large owner to one warp
+      // can only lengthen the run's tail
+      int cta = kOut / 2;
       for (int k = kOut / 2 + 1; k < kOut; ++k)
         if (y[k] < y[cta]) cta = k;
+      int best = cta;
+      if (roff[x + 1] - roff[x] <= kRankCtaMin)
+        for (int k = 0; k < kOut / 2; ++k)
+          if (y[k] < y[best]) best = k;
       const float cost = exp2f(y[best]) - 1.f;
       cfg[x] = (uint8_t)best;
       warp_cost[t] = best < kOut / 2 ? cost : 0.f;

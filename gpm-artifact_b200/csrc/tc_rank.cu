@@ -622,9 +622,53 @@ int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long l
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
   if (g->nnz == 0) return cudaMemsetAsync(d_out, 0, 8, st) == cudaSuccess ? GPM_OK : GPM_ECUDA;
   // fixed schedule: owners with > kRankCtaMin keys go to a CTA, segments of
-  // >= kRankLongMin keys are streamed by a whole warp
+  // >= kRankLongMin keys are streamed by a half-warp
   GPM_TRY(rank_build_plan(g, kRankCtaMin, kRankLongMin, st));
   return rank_plan_launch(g, g->rank, st, d_out, nullptr);
 }
 
+// out[0] segments, out[1] keys in them, out[2] keys of the owners' lists
+__global__ void k_plan_stats(int64_t nseg, const longlong2 *__restrict__ pseg, const int32_t *__restrict__ tasks,
+                             int ntasks, const int64_t *__restrict__ roff, unsigned long long *__restrict__ out) {
+  unsigned long long keys = 0, okeys = 0;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nseg; j += (int64_t)gridDim.x * blockDim.x)
+    keys += (unsigned long long)(pseg[j].y - pseg[j].x);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntasks; t += (int64_t)gridDim.x * blockDim.x)
+    okeys += (unsigned long long)(roff[tasks[t] + 1] - roff[tasks[t]]);
+  keys = warp_sum(keys);
+  okeys = warp_sum(okeys);
+  if (lane_id() == 0) {
+    atomicAdd(&out[1], keys);
+    atomicAdd(&out[2], okeys);
+  }
+}
+
+int rank_plan_stats(gpm_graph *g, uint64_t *out) {
+  out[0] = out[1] = out[2] = out[3] = 0;
+  if (g->nnz == 0) return GPM_OK;
+  GPM_TRY(rank_build_plan(g, kRankCtaMin, kRankLongMin, 0));
+  RankPlan *p = g->rank;
+  int64_t nseg = 0;
+  GPM_CUDA(cudaMemcpy(&nseg, p->poff.p + g->n, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  DevBuf<unsigned long long> o;
+  GPM_TRY(o.reserve(3));
+  GPM_CUDA(cudaMemset(o.p, 0, 24));
+  const int grid = num_sms() * 8;
+  k_plan_stats<<<grid, 256>>>(nseg, p->pseg.p, p->cta_tasks.p, p->n_cta, g->rg->roff.p, o.p);
+  k_plan_stats<<<grid, 256>>>(0, p->pseg.p, p->warp_tasks.p, p->n_warp, g->rg->roff.p, o.p);
+  GPM_LAUNCH_CHECK();
+  unsigned long long h[3];
+  GPM_CUDA(cudaMemcpy(h, o.p, sizeof h, cudaMemcpyDeviceToHost));
+  out[0] = (uint64_t)nseg;
+  out[1] = h[1];
+  out[2] = h[2];
+  out[3] = (uint64_t)(p->n_cta + p->n_warp);
+  return GPM_OK;
+}
+
 }  // namespace gpm
+
+extern "C" int gpm_tc_plan_stats(gpm_graph *g, uint64_t *stats) {
+  if (!g || !stats) return gpm::fail(GPM_EINVAL, "gpm_tc_plan_stats: NULL argument");
+  return gpm::rank_plan_stats(g, stats);
+}

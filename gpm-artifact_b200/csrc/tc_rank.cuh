@@ -59,6 +59,8 @@ int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid = nullpt
                       bool upward_only = false);
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st);
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out);
+// out[0..3]: segments, keys in them, owner-list keys, owner tasks of the fixed plan
+int rank_plan_stats(gpm_graph *g, uint64_t *out);
 // An uncached plan; cfg (device, one byte per vertex, may be nullptr) gives
 // each owner its queue (cfg / 3: 0 warp, 1 CTA) and long-segment threshold
 // ({16, 64, 256}[cfg % 3]) instead of the fixed thresholds.

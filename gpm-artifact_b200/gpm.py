@@ -64,6 +64,7 @@ _SIGS = {
     "gpm_tc": ([_P, c_int, POINTER(c_uint64)], c_int),
     "gpm_tc_async": ([_P, c_int, _P, _P], c_int),
     "gpm_tc_host_csr": ([c_int64, _P, _P, c_int, _P, POINTER(c_uint64)], c_int),
+    "gpm_tc_plan_stats": ([_P, _P], c_int),
     "gpm_tc_csr_noalloc": ([c_int64, _P, _P, _P, _P], c_int),
     "gpm_clique": ([_P, c_int, POINTER(c_uint64)], c_int),
     "gpm_clique_ex": ([_P, c_int, c_int, POINTER(c_uint64)], c_int),
@@ -250,6 +251,13 @@ class Graph:
         w, p = c_uint64(), c_uint64()
         check(lib.gpm_graph_work(self.h, ctypes.byref(w), ctypes.byref(p)))
         return w.value, p.value
+
+    def plan_stats(self):
+        """(segments, streamed keys, owner keys, owner tasks) of the fixed
+        GPM_TC_BITMAP plan."""
+        st = np.zeros(4, np.uint64)
+        check(lib.gpm_tc_plan_stats(self.h, _ptr(st)))
+        return tuple(int(x) for x in st)
 
     def tc(self, mode=V_CENTRIC) -> int:
         out = c_uint64()

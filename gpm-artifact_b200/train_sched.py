@@ -1,6 +1,7 @@
 """Trains the learned task scheduler's shipped parameters (sched_tc.f32).
 
     python gpm-artifact_b200/train_sched.py [--out PATH] [--steps 1500] [--lr 3e-3]
+    python gpm-artifact_b200/train_sched.py --eval-only
 
 Training graphs (the R-MAT scale-22 benchmark graph is not among them):
 R-MAT scales 15, 16, 17, 18 (edge factor 16, seeds 11, 12, 13, 21) and two
@@ -74,7 +75,11 @@ def main():
     ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--no-eval", action="store_true")
+    ap.add_argument("--eval-only", action="store_true", help="evaluate the shipped parameters, no training")
     a = ap.parse_args()
+    if a.eval_only:
+        held_out(gpm.Sched.pretrained())
+        return
     s, rows, first, last = train(a.steps, a.lr)
     s.params().astype(np.float32).tofile(a.out)
     print(json.dumps({"rows": rows, "loss_first": first, "loss_last": last, "out": a.out}), flush=True)

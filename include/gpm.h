@@ -164,6 +164,11 @@ int gpm_tc_async(gpm_graph *g, int variant, void *stream, uint64_t *d_out);
  * the RunTC path as one call.  stream may be NULL. */
 int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, int variant,
                     void *stream, uint64_t *out);
+/* Work of GPM_TC_BITMAP's fixed plan on g (built if needed), no reference
+ * counterpart: stats[0] partner segments, stats[1] keys streamed from them,
+ * stats[2] keys of the owner lists loaded into shared memory, stats[3] owner
+ * tasks. */
+int gpm_tc_plan_stats(gpm_graph *g, uint64_t *stats);
 
 /* Triangle count of a device-resident CSR that allocates nothing -- this
  * entry point has no counterpart in the reference.  It serves callers that
@@ -211,8 +216,9 @@ int gpm_pattern(gpm_graph *g, const char *name, int family, uint64_t *counters,
  * Each owner task of GPM_TC_BITMAP gets one of 6 configurations:
  * queue (cfg / 3: 0 warp, 1 CTA) x long-segment threshold ({16, 64, 256}[cfg % 3]).
  * A 3-layer FP32 MLP (8 -> 32 -> 32 -> 6) predicts log2 active warp-cycles of
- * each configuration from 8 task features; a task takes its cheapest one,
- * except that a warp-queue task predicted to cost more than half a warp
+ * each configuration from 8 task features; a task takes its cheapest one
+ * (owners above the fixed schedule's CTA threshold choose among the CTA
+ * configurations only), except that a warp-queue task predicted to cost more than half a warp
  * slot's share of the total takes its cheapest CTA configuration.  Counts
  * never depend on the choice. */
 int gpm_sched_create(uint64_t seed, gpm_sched **out);

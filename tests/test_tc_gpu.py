@@ -120,3 +120,48 @@ def test_host_csr_end_to_end():
     want = orc.tc(doff, didx)
     for v in VARIANTS:
         assert gpm.tc_host_csr(off, idx, v) == want
+
+
+def plan_numpy(off, idx):
+    """The fixed plan's work restated in numpy: rank by (degree, id), DAG
+    edges upward, owner = endpoint with the longer out-list (ties to the
+    source), segment = the partner's list clipped to [min, max] of the
+    owner's list (owners with fewer than 2 keys have none)."""
+    n = len(off) - 1
+    deg = np.diff(off)
+    order = np.lexsort((np.arange(n), deg))
+    rank = np.empty(n, np.int64)
+    rank[order] = np.arange(n)
+    rs, rd = rank[np.repeat(np.arange(n), deg)], rank[idx]
+    up = rd > rs
+    us, vs = rs[up], rd[up]
+    o = np.lexsort((vs, us))
+    us, vs = us[o], vs[o]
+    dp = np.bincount(us, minlength=n)
+    roff = np.zeros(n + 1, np.int64)
+    roff[1:] = np.cumsum(dp)
+    du, dv = dp[us], dp[vs]
+    own_u = dv <= du
+    owner, partner = np.where(own_u, us, vs), np.where(own_u, vs, us)
+    kmin = vs[np.minimum(roff[:-1], len(vs) - 1)]
+    kmax = vs[np.maximum(roff[1:] - 1, 0)]
+    key = us * (n + 1) + vs
+    a = np.searchsorted(key, partner * (n + 1) + kmin[owner], "left")
+    b = np.searchsorted(key, partner * (n + 1) + kmax[owner], "right")
+    clip = np.where(np.maximum(du, dv) >= 2, np.maximum(b - a, 0), 0)
+    seg = clip > 0
+    tasks = np.unique(owner[seg])
+    return int(seg.sum()), int(clip.sum()), int(dp[tasks].sum()), len(tasks)
+
+
+@pytest.mark.parametrize("kind", ["rmat", "er"])
+def test_plan_segments_match_numpy(kind):
+    """The plan streams exactly the clipped segments: their number, their
+    keys, the owner keys and the owner tasks equal the numpy restatement."""
+    if kind == "rmat":
+        n, s, d = gpm.gen_rmat(13, 16, seed=7)
+    else:
+        n, s, d = gpm.gen_er(20000, 300000, seed=7)
+    off, idx = orc.build_csr(n, s, d)
+    g = gpm.Graph.from_csr(off, idx).orient()
+    assert g.plan_stats() == plan_numpy(off, idx)
