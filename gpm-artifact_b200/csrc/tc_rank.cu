@@ -25,6 +25,8 @@
 // step; short ones by 8-lane groups.  Owners with more than `cta_min` keys
 // are CTA tasks, the rest warp tasks; both queues are sorted heaviest first
 // and drained by a persistent grid.
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -34,6 +36,8 @@
 #include "tc_rank.cuh"
 
 namespace gpm {
+
+namespace cg = cooperative_groups;
 
 constexpr int kRWarps = 8;
 constexpr int kCtaWords = kRankCtaWords;
@@ -240,11 +244,12 @@ __global__ void k_indeg(int64_t nnz, const int32_t *__restrict__ adj, int32_t *_
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnz; i += (int64_t)gridDim.x * blockDim.x)
     atomicAdd(&indeg[adj[i]], 1);
 }
-// sort key: (graph id, in + out degree); the stable sort breaks ties by id
+// sort key: (graph id, in + out degree); the stable sort breaks ties by id.
+// indeg == nullptr: the stored graph is symmetric, out-degree orders alike
 __global__ void k_rank_keys(int64_t n, const int64_t *__restrict__ off, const int32_t *__restrict__ indeg,
                             const int32_t *__restrict__ gid, uint64_t *__restrict__ key, int32_t *__restrict__ val) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t d = (uint64_t)(uint32_t)((off[i + 1] - off[i]) + indeg[i]);
+    uint64_t d = (uint64_t)(uint32_t)((off[i + 1] - off[i]) + (indeg ? indeg[i] : 0));
     key[i] = gid ? ((uint64_t)(uint32_t)gid[i] << 32) | d : d;
     val[i] = (int32_t)i;
   }
@@ -257,16 +262,99 @@ __global__ void k_rank_inverse(int64_t n, const int32_t *__restrict__ order, con
     rdeg[r] = off[v + 1] - off[v];
   }
 }
-__global__ void k_rank_copy(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ rank,
-                            const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
-                            const int64_t *__restrict__ roff, int32_t *__restrict__ out) {
-  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+// Relabelled lists, gathered and sorted in one pass (one warp per rank r):
+// the neighbours of order[r] as ranks (UPWARD: only ranks above r, the
+// degree-oriented DAG of a symmetric graph, graph.h:128-129) are compacted
+// into the warp's shared buffer, sorted there -- a register bitonic network
+// up to 32 keys, a shared-memory one up to kSortCap -- and written to
+// out[roff[r] ..].  Longer lists are written unsorted and their rank
+// appended to big[] for a segmented sort afterwards.
+constexpr int kSortCap = 1024;
+constexpr int kGatherWarps = 8;
+
+__device__ __forceinline__ int32_t warp_bitonic32(int32_t key, unsigned lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const int32_t other = __shfl_xor_sync(0xffffffffu, key, j);
+      const bool asc = (lane & k) == 0, low = (lane & j) == 0;
+      key = (low == asc) ? min(key, other) : max(key, other);
+    }
+  return key;
+}
+
+template <bool UPWARD>
+__global__ void __launch_bounds__(kGatherWarps * 32)
+    k_rank_gather_sort(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ rank,
+                       const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                       const int64_t *__restrict__ roff, int32_t *__restrict__ out, int32_t *__restrict__ big,
+                       int *__restrict__ nbig) {
+  __shared__ int32_t sbuf[kGatherWarps][kSortCap];
+  int32_t *buf = sbuf[threadIdx.x >> 5];
+  const unsigned lane = lane_id();
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = warp; r < n; r += nw) {
-    int32_t v = order[r];
-    int64_t s = off[v], e = off[v + 1], o = roff[r];
-    for (int64_t k = s + lane_id(); k < e; k += 32) out[o + (k - s)] = rank[adj[k]];
+    const int32_t v = order[r];
+    const int64_t s = off[v], e = off[v + 1], o = roff[r];
+    const int64_t len = roff[r + 1] - o;
+    if (len == 0) continue;
+    const bool fits = len <= kSortCap;
+    int32_t *dst = fits ? buf : out + o;
+    int64_t filled = 0;
+    for (int64_t base = s; base < e && filled < len; base += 32) {
+      const int64_t k = base + lane;
+      const int32_t x = k < e ? rank[adj[k]] : -1;
+      const bool keep = k < e && (!UPWARD || x > (int32_t)r);
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (keep) dst[filled + __popc(m & ((1u << lane) - 1u))] = x;
+      filled += __popc(m);
+    }
+    __syncwarp();
+    if (!fits) {
+      if (lane == 0) big[atomicAdd(nbig, 1)] = (int32_t)r;
+      continue;
+    }
+    if (len <= 32) {
+      const int32_t key = warp_bitonic32((int64_t)lane < len ? buf[lane] : INT_MAX, lane);
+      if ((int64_t)lane < len) out[o + lane] = key;
+    } else {
+      int p = 64;
+      while (p < len) p <<= 1;
+      for (int i = (int)len + lane; i < p; i += 32) buf[i] = INT_MAX;
+      __syncwarp();
+      for (int k = 2; k <= p; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          for (int i = lane; i < p; i += 32) {
+            const int ixj = i ^ j;
+            if (ixj > i) {
+              const int32_t a = buf[i], b = buf[ixj];
+              if ((a > b) == ((i & k) == 0)) {
+                buf[i] = b;
+                buf[ixj] = a;
+              }
+            }
+          }
+          __syncwarp();
+        }
+      for (int64_t i = lane; i < len; i += 32) out[o + i] = buf[i];
+    }
+    __syncwarp();
   }
+}
+
+__global__ void k_big_bounds(int nbig, const int32_t *__restrict__ big, const int64_t *__restrict__ roff,
+                             int64_t *__restrict__ bb, int64_t *__restrict__ be) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbig; i += gridDim.x * blockDim.x) {
+    bb[i] = roff[big[i]];
+    be[i] = roff[big[i] + 1];
+  }
+}
+__global__ void k_big_copy(int nbig, const int64_t *__restrict__ bb, const int64_t *__restrict__ be,
+                           const int32_t *__restrict__ src, int32_t *__restrict__ dst) {
+  for (int i = blockIdx.x; i < nbig; i += gridDim.x)
+    for (int64_t k = bb[i] + threadIdx.x; k < be[i]; k += blockDim.x) dst[k] = src[k];
 }
 
 // Orientation folded into the relabel: keep only neighbours of larger rank
@@ -284,26 +372,6 @@ __global__ void k_rank_up_count(int64_t n, const int32_t *__restrict__ order, co
     if (lane_id() == 0) rdeg[r] = c;
   }
 }
-__global__ void k_rank_up_copy(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ rank,
-                               const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
-                               const int64_t *__restrict__ roff, int32_t *__restrict__ out) {
-  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const unsigned lane = lane_id();
-  for (int64_t r = warp; r < n; r += nw) {
-    int32_t v = order[r];
-    int64_t s = off[v], e = off[v + 1], w = roff[r];
-    for (int64_t base = s; base < e; base += 32) {
-      int64_t k = base + lane;
-      int32_t x = k < e ? rank[adj[k]] : -1;
-      bool keep = x > (int32_t)r;
-      unsigned m = __ballot_sync(0xffffffffu, keep);
-      if (keep) out[w + __popc(m & ((1u << lane) - 1u))] = x;
-      w += __popc(m);
-    }
-  }
-}
-
 // Per-owner task configuration (learned scheduler): queue = cfg / 3
 // (0 warp, 1 CTA), long-segment threshold = kCfgLong[cfg % 3].
 __device__ __constant__ int kCfgLong[3] = {16, 64, 256};
@@ -339,10 +407,15 @@ __device__ __forceinline__ int64_t upper_bound_key(const int32_t *__restrict__ a
 // partner's list inside [min, max] of the owner's list; its start and length
 // go to sstart[k] / slen[k] (length 0: nothing to stream, also when the
 // owner has fewer than 2 keys and so closes no triangle through the edge).
+// upward: every list holds only ids above its vertex, so when u owns the
+// edge, min N(u) <= v < every id of N(v) and the lower search is skipped.
+// Per-owner counters take one atomic per (owner, class) and warp, the lanes
+// of a warp that share them combined first (hub owners get most of theirs
+// from their own list, i.e. from one warp).
 __global__ void k_partner_count(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                                int long_min, const uint8_t *__restrict__ cfg, int32_t *__restrict__ nlong,
-                                int32_t *__restrict__ nshort, int64_t *__restrict__ sstart,
-                                int32_t *__restrict__ slen) {
+                                int upward, int long_min, const uint8_t *__restrict__ cfg,
+                                int32_t *__restrict__ nlong, int32_t *__restrict__ nshort,
+                                int64_t *__restrict__ sstart, int32_t *__restrict__ slen) {
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = warp; u < n; u += nw) {
@@ -356,12 +429,17 @@ __global__ void k_partner_count(int64_t n, const int64_t *__restrict__ roff, con
       int64_t ps = own_u ? vs : s, pe = own_u ? ve : e;
       int64_t lo = 0, len = 0;
       if (oe - os >= 2) {
-        lo = lower_bound_key(radj, ps, pe, radj[os]);
+        lo = upward && own_u ? ps : lower_bound_key(radj, ps, pe, radj[os]);
         len = upper_bound_key(radj, lo, pe, radj[oe - 1]) - lo;
       }
       sstart[k] = lo;
       slen[k] = (int32_t)len;
-      if (len > 0) atomicAdd(len >= owner_long_min(cfg, owner, long_min) ? &nlong[owner] : &nshort[owner], 1);
+      if (len > 0) {
+        const bool lng = len >= owner_long_min(cfg, owner, long_min);
+        cg::coalesced_group grp =
+            cg::labeled_partition(cg::coalesced_threads(), ((unsigned long long)(uint32_t)owner << 1) | lng);
+        if (grp.thread_rank() == 0) atomicAdd(lng ? &nlong[owner] : &nshort[owner], (int)grp.size());
+      }
     }
   }
 }
@@ -391,11 +469,16 @@ __global__ void k_partner_fill(int64_t n, const int64_t *__restrict__ roff, cons
       if (len == 0) continue;
       int32_t v = radj[k];
       int32_t owner = roff[v + 1] - roff[v] <= du ? (int32_t)u : v;
-      unsigned long long pos =
-          atomicAdd(len >= owner_long_min(cfg, owner, long_min) ? &curl[owner] : &curs[owner], 1ull);
+      const bool lng = len >= owner_long_min(cfg, owner, long_min);
+      cg::coalesced_group grp =
+          cg::labeled_partition(cg::coalesced_threads(), ((unsigned long long)(uint32_t)owner << 1) | lng);
+      unsigned long long pos = 0;
+      if (grp.thread_rank() == 0) pos = atomicAdd(lng ? &curl[owner] : &curs[owner], (unsigned long long)grp.size());
+      pos = grp.shfl(pos, 0) + grp.thread_rank();
       const int64_t lo = sstart[k];
       pseg[pos] = make_longlong2(lo, lo + len);
-      atomicAdd(&work[owner], (unsigned long long)len + 1ull);
+      const unsigned long long w = cg::reduce(grp, (unsigned long long)len + 1ull, cg::plus<unsigned long long>());
+      if (grp.thread_rank() == 0) atomicAdd(&work[owner], w);
     }
   }
 }
@@ -479,9 +562,13 @@ int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid, int ngr
   int end_bit = 32;
   if (gid)
     while (end_bit < 64 && (1ll << (end_bit - 32)) < ngraphs) ++end_bit;
-  cudaMemsetAsync(indeg.p, 0, sizeof(int32_t) * n, st);
-  k_indeg<<<grid_for(nnz), 256, 0, st>>>(nnz, g->adj.p, indeg.p);
-  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, indeg.p, gid, key.p, val.p);
+  // upward_only takes a symmetric graph, whose in-degrees equal its
+  // out-degrees: the key needs no in-degree pass then
+  if (!upward_only) {
+    cudaMemsetAsync(indeg.p, 0, sizeof(int32_t) * n, st);
+    k_indeg<<<grid_for(nnz), 256, 0, st>>>(nnz, g->adj.p, indeg.p);
+  }
+  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, upward_only ? nullptr : indeg.p, gid, key.p, val.p);
   {
     size_t tmp = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, val.p, order, (int)n, 0, end_bit, st);
@@ -498,19 +585,35 @@ int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid, int ngr
     cudaStreamSynchronize(st);
   }
   {
-    DevBuf<int32_t> tmpadj;
-    if ((s = tmpadj.reserve(nnz))) return bail(s);
+    // gather + sort in one pass; lists longer than kSortCap get a segmented
+    // sort of their own afterwards
+    DevBuf<int32_t> big;
+    DevBuf<int> nbig;
+    if ((s = big.reserve(n)) || (s = nbig.reserve(1))) return bail(s);
+    cudaMemsetAsync(nbig.p, 0, sizeof(int), st);
+    const int ggrid = grid_for(n * 32, kGatherWarps * 32);
     if (upward_only)
-      k_rank_up_copy<<<grid_for(n * 32), 256, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, r->roff.p, tmpadj.p);
+      k_rank_gather_sort<true><<<ggrid, kGatherWarps * 32, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, r->roff.p,
+                                                                    r->radj.p, big.p, nbig.p);
     else
-      k_rank_copy<<<grid_for(n * 32), 256, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, r->roff.p, tmpadj.p);
-    size_t tmp = 0;
-    cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, tmpadj.p, r->radj.p, (int)nnz, (int)n, r->roff.p,
-                                       r->roff.p + 1, st);
-    DevBuf<char> t;
-    if ((s = t.reserve(tmp))) return bail(s);
-    cub::DeviceSegmentedSort::SortKeys(t.p, tmp, tmpadj.p, r->radj.p, (int)nnz, (int)n, r->roff.p,
-                                       r->roff.p + 1, st);
+      k_rank_gather_sort<false><<<ggrid, kGatherWarps * 32, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p,
+                                                                     r->roff.p, r->radj.p, big.p, nbig.p);
+    int hbig = 0;
+    cudaMemcpyAsync(&hbig, nbig.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank relabel: ") + cudaGetErrorString(e)));
+    if (hbig > 0) {
+      DevBuf<int64_t> bb, be;
+      DevBuf<int32_t> sorted;
+      if ((s = bb.reserve(hbig)) || (s = be.reserve(hbig)) || (s = sorted.reserve(nnz))) return bail(s);
+      k_big_bounds<<<grid_for(hbig), 256, 0, st>>>(hbig, big.p, r->roff.p, bb.p, be.p);
+      size_t tmp = 0;
+      cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, r->radj.p, sorted.p, (int)nnz, hbig, bb.p, be.p, st);
+      DevBuf<char> t;
+      if ((s = t.reserve(tmp))) return bail(s);
+      cub::DeviceSegmentedSort::SortKeys(t.p, tmp, r->radj.p, sorted.p, (int)nnz, hbig, bb.p, be.p, st);
+      k_big_copy<<<std::min(hbig, num_sms() * 8), 256, 0, st>>>(hbig, bb.p, be.p, sorted.p, r->radj.p);
+    }
   }
   // does every stored edge point to a larger rank? (true for a degree-oriented DAG)
   cudaMemsetAsync(down.p, 0, sizeof(int), st);
@@ -560,8 +663,8 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
   cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(nshort.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
-  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, cfg, p->plong.p, nshort.p,
-                                                     sstart.p, slen.p);
+  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, g->rg->upward, long_min, cfg, p->plong.p,
+                                                     nshort.p, sstart.p, slen.p);
   k_partner_sizes<<<grid_for(n), 256, 0, st>>>(n, p->plong.p, nshort.p, tot.p);
   if ((s = scan_i64(n, tot.p, p->poff.p, st))) return bail(s);
   k_partner_cursors<<<grid_for(n), 256, 0, st>>>(n, p->poff.p, p->plong.p, curl.p, curs.p);

@@ -83,3 +83,18 @@ def test_unknown_pattern():
     with pytest.raises(gpm.GpmError) as e:
         g.pattern("P9")
     assert e.value.status == 1
+
+
+def test_hub_lists_longer_than_the_sort_buffer():
+    """A 3999-leaf hub: its relabelled list (3999 ids) is beyond the
+    1024-key sort buffer of the relabel and takes the segmented-sort
+    fallback; the motif counts stay exact."""
+    n = 4000
+    rng = np.random.default_rng(11)
+    other = rng.integers(1, n, size=(30000, 2))
+    s = np.concatenate([np.zeros(n - 1, np.int64), other[:, 0]]).astype(np.int32)
+    d = np.concatenate([np.arange(1, n), other[:, 1]]).astype(np.int32)
+    off, idx = sym(n, s, d)
+    assert np.diff(off).max() > 1024
+    g = gpm.Graph.from_edges(n, s, d)
+    assert g.motif(4).tolist() == orc.motif4(off, idx).tolist()

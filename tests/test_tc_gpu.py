@@ -165,3 +165,21 @@ def test_plan_segments_match_numpy(kind):
     off, idx = orc.build_csr(n, s, d)
     g = gpm.Graph.from_csr(off, idx).orient()
     assert g.plan_stats() == plan_numpy(off, idx)
+
+
+def test_lists_longer_than_the_sort_buffer():
+    """Relabelled lists longer than the 1024-key sort buffer take the
+    segmented-sort fallback: a 1200-clique (DAG out-lists up to 1199) with a
+    sparse random fringe, through the oriented graph and the host-CSR path."""
+    n = 5000
+    iu, ju = np.triu_indices(1200, 1)
+    fr = np.random.default_rng(3).integers(0, n, size=(20000, 2))
+    s = np.concatenate([iu, fr[:, 0]]).astype(np.int32)
+    d = np.concatenate([ju, fr[:, 1]]).astype(np.int32)
+    off, idx, doff, didx = oracle_graph(n, s, d)
+    assert np.diff(doff).max() > 1024
+    want = orc.tc(doff, didx)
+    g = gpm.Graph.from_edges(n, s, d).orient()
+    assert tc_all_variants(g) == [want] * len(VARIANTS)
+    assert gpm.tc_host_csr(off, idx, gpm.TC_AUTO) == want
+    assert g.plan_stats() == plan_numpy(off, idx)
