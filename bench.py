@@ -44,7 +44,7 @@ A, B, C = 0.57, 0.19, 0.19
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100, help="timed counts (100 x ~7 ms: long enough to sample clocks)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (22 is the headline workload)")
