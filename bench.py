@@ -52,6 +52,7 @@ def parse():
                     choices=["auto", "bitmap", "hash", "bsearch", "merge", "learned"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="reference arm: skip the reference's GPU solvers")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample time")
     return ap.parse_args()
 
@@ -337,9 +338,58 @@ def main():
         dist.destroy_process_group()
 
 
+def reference_gpu(off, idx, m_und, timeout=600):
+    """The reference's own GPU triangle count of the same graph, for the
+    record: its e-centric (test_engine) and v-centric (test_trianglecounting)
+    drivers, compiled for sm_100a from its sources into oracle/_ref, each
+    timed by its own kernel-window line "Triangle counting  time: X seconds"
+    (src/TCSolver.cuh:26,61-63,108-113).  The reference's .mtx loader sizes
+    the graph from the ids present, so isolated vertices are dropped first
+    (an order-preserving renumbering: same orientation, same count)."""
+    import re
+    import tempfile
+    import numpy as np
+    import _oracle as orc
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    drivers = {"e_centric": ("test_engine", r"Result: (\d+)"),
+               "v_centric": ("test_trianglecounting", r"Pattern 0: (\d+)")}
+    if not all(os.path.exists(os.path.join(ref, d)) for d, _ in drivers.values()):
+        return {"unavailable": "reference GPU drivers not built (make -C oracle refgpu where the reference is mounted)"}
+    deg = np.diff(off)
+    live = np.nonzero(deg)[0]
+    remap = np.full(len(deg), -1, np.int64)
+    remap[live] = np.arange(len(live))
+    off2 = np.zeros(len(live) + 1, np.int64)
+    off2[1:] = np.cumsum(deg[live])
+    idx2 = remap[idx].astype(np.int32)
+    res = {"graph": f"{len(live)} non-isolated vertices, {m_und} edges"}
+    with tempfile.TemporaryDirectory() as td:
+        mtx, lab = os.path.join(td, "g.mtx"), os.path.join(td, "g.lab")
+        orc.write_mtx(mtx, off2, idx2)
+        with open(lab, "w") as f:
+            f.write("".join(f"{v} 1\n" for v in range(1, len(live) + 1)))
+        for mode, (drv, pat) in drivers.items():
+            argv = [os.path.join(ref, drv), mtx] + ([lab] if drv == "test_engine" else [])
+            try:
+                out = subprocess.run(argv, capture_output=True, text=True, timeout=timeout)
+            except subprocess.TimeoutExpired:
+                res[mode] = {"unavailable": f"no result within {timeout} s"}
+                continue
+            t = re.findall(r"Triangle counting\s+time:\s*([0-9.eE+-]+)\s*seconds", out.stdout)
+            c = re.findall(pat, out.stdout)
+            if out.returncode != 0 or not t or not c:
+                res[mode] = {"unavailable": f"exit {out.returncode}, no time/result line"}
+                continue
+            sec = float(t[-1])
+            res[mode] = {"ms": sec * 1e3, "triangles": int(c[-1]), "teps": m_und / sec}
+    return res
+
+
 def reference_arm(args, rank, world, dist):
     """The reference has no CPU triangle counter of its own; its arm is the
-    CPU restatement of its algorithm (oracle port) on all host threads."""
+    CPU restatement of its algorithm (oracle port) on all host threads.  Each
+    step is a vertex sample sized so that all steps take about 90 s.  Beside
+    it, the reference's own GPU solvers on the same graph (reference_gpu)."""
     import numpy as np
     if rank != 0:
         if dist:
@@ -354,8 +404,9 @@ def reference_arm(args, rank, world, dist):
     threads = len(os.sched_getaffinity(0))
     vals = []
     sample = ""
+    per_step = min(args.cpu_seconds, 8.0, 90.0 / (max(args.warmup, 3) + args.steps))
     for k in range(max(args.warmup, 3) + args.steps):
-        v, sample = cpu_sample(doff, didx, m_und, min(args.cpu_seconds, 8.0), threads)
+        v, sample = cpu_sample(doff, didx, m_und, per_step, threads)
         if k >= max(args.warmup, 3):
             vals.append(v)
     value = statistics.median(vals)
@@ -367,6 +418,8 @@ def reference_arm(args, rank, world, dist):
                        "edge_factor": EF, "parallelism": "cpu"},
             "cpu_baseline": {"value": value, "unit": "TEPS", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "TEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_ref_gpu:
+        line["reference_gpu"] = reference_gpu(off, idx, m_und)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -18,6 +18,7 @@
  */
 #include "gpm_oracle.h"
 
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -709,5 +710,54 @@ uint64_t orc_tc_tasks(int64_t n, const int64_t *doff, const int32_t *didx, const
     }
     free(mark);
   }
+  return total;
+}
+
+/* Writes a CSR as the Matrix Market coordinate text the reference's loader
+ * reads (src/graph/io.h:22-153): a "rows cols entries" line, then one
+ * 1-indexed "u v" line per stored entry.  Used to hand the same graph to the
+ * reference's own solvers.  Returns the bytes written, -1 on an I/O error. */
+static char *put_u64(char *p, uint64_t v) {
+  char t[24];
+  int k = 0;
+  do {
+    t[k++] = (char)('0' + v % 10);
+    v /= 10;
+  } while (v);
+  while (k) *p++ = t[--k];
+  return p;
+}
+
+int64_t orc_write_mtx(const char *path, int64_t n, const int64_t *off, const int32_t *idx) {
+  FILE *f = fopen(path, "wb");
+  if (!f) return -1;
+  const size_t cap = (size_t)1 << 22;
+  char *buf = (char *)malloc(cap + 64);
+  char *p = buf;
+  int64_t total = 0, u, e;
+  p = put_u64(p, (uint64_t)n);
+  *p++ = ' ';
+  p = put_u64(p, (uint64_t)n);
+  *p++ = ' ';
+  p = put_u64(p, (uint64_t)off[n]);
+  *p++ = '\n';
+  for (u = 0; u < n; u++)
+    for (e = off[u]; e < off[u + 1]; e++) {
+      p = put_u64(p, (uint64_t)u + 1);
+      *p++ = ' ';
+      p = put_u64(p, (uint64_t)idx[e] + 1);
+      *p++ = '\n';
+      if ((size_t)(p - buf) >= cap) {
+        if (fwrite(buf, 1, (size_t)(p - buf), f) != (size_t)(p - buf)) total = -1;
+        if (total >= 0) total += p - buf;
+        p = buf;
+      }
+    }
+  if (p > buf) {
+    if (fwrite(buf, 1, (size_t)(p - buf), f) != (size_t)(p - buf)) total = -1;
+    if (total >= 0) total += p - buf;
+  }
+  free(buf);
+  if (fclose(f) != 0) total = -1;
   return total;
 }

@@ -70,6 +70,10 @@ void orc_motif_bruteforce(int64_t n, const int64_t *off, const int32_t *idx, uin
  * (sub_ceci/myceci.cpp:540-668): the number of injective, label-preserving
  * maps of the query vertices into the data graph that map every query edge to
  * a data edge (non-induced; automorphic images counted separately). */
+/* The CSR as 1-indexed Matrix Market coordinate text (the reference
+ * loader's input, src/graph/io.h:22-153); bytes written or -1. */
+int64_t orc_write_mtx(const char *path, int64_t n, const int64_t *off, const int32_t *idx);
+
 uint64_t orc_match(int64_t n, const int64_t *off, const int32_t *idx, const int32_t *labels,
                    int64_t qn, const int64_t *qoff, const int32_t *qidx,
                    const int32_t *qlabels, int threads);

@@ -26,6 +26,7 @@ def lib():
             getattr(L, f).restype = c_uint64
         L.orc_build_csr.restype = c_int64
         L.orc_orient.restype = c_int64
+        L.orc_write_mtx.restype = c_int64
         _lib = L
     return _lib
 
@@ -106,3 +107,13 @@ def motif3(off, idx, tri):
     d = np.diff(off).astype(np.uint64)
     wedges = int(np.sum(d * (d - np.uint64(1)) // np.uint64(2))) if len(d) else 0
     return np.array([wedges - 3 * tri, tri], np.uint64)
+
+
+def write_mtx(path, off, idx):
+    """The CSR as 1-indexed Matrix Market text for the reference's loader."""
+    off = np.ascontiguousarray(off, np.int64)
+    idx = np.ascontiguousarray(idx, np.int32)
+    r = lib().orc_write_mtx(str(path).encode(), c_int64(len(off) - 1), _p(off), _p(idx))
+    if r < 0:
+        raise OSError(f"writing {path} failed")
+    return r
