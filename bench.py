@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="reference arm: skip the reference's GPU solvers")
+    ap.add_argument("--ref-extra", default="", help="reference arm: also time the reference's GPU solvers on "
+                    "'clique' (R-MAT 20, k = 4, 5) and/or 'motif' (R-MAT 18, Motif4); one more JSON line")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample time")
     return ap.parse_args()
 
@@ -355,19 +357,13 @@ def reference_gpu(off, idx, m_und, timeout=600):
                "v_centric": ("test_trianglecounting", r"Pattern 0: (\d+)")}
     if not all(os.path.exists(os.path.join(ref, d)) for d, _ in drivers.values()):
         return {"unavailable": "reference GPU drivers not built (make -C oracle refgpu where the reference is mounted)"}
-    deg = np.diff(off)
-    live = np.nonzero(deg)[0]
-    remap = np.full(len(deg), -1, np.int64)
-    remap[live] = np.arange(len(live))
-    off2 = np.zeros(len(live) + 1, np.int64)
-    off2[1:] = np.cumsum(deg[live])
-    idx2 = remap[idx].astype(np.int32)
-    res = {"graph": f"{len(live)} non-isolated vertices, {m_und} edges"}
+    off2, idx2 = _compact_csr(off, idx)
+    res = {"graph": f"{len(off2) - 1} non-isolated vertices, {m_und} edges"}
     with tempfile.TemporaryDirectory() as td:
         mtx, lab = os.path.join(td, "g.mtx"), os.path.join(td, "g.lab")
         orc.write_mtx(mtx, off2, idx2)
         with open(lab, "w") as f:
-            f.write("".join(f"{v} 1\n" for v in range(1, len(live) + 1)))
+            f.write("".join(f"{v} 1\n" for v in range(1, len(off2))))
         for mode, (drv, pat) in drivers.items():
             argv = [os.path.join(ref, drv), mtx] + ([lab] if drv == "test_engine" else [])
             try:
@@ -382,6 +378,66 @@ def reference_gpu(off, idx, m_und, timeout=600):
                 continue
             sec = float(t[-1])
             res[mode] = {"ms": sec * 1e3, "triangles": int(c[-1]), "teps": m_und / sec}
+    return res
+
+
+def _compact_csr(off, idx):
+    """Isolated vertices dropped by an order-preserving renumbering (the
+    reference's .mtx loader sizes the graph from the ids present)."""
+    import numpy as np
+    deg = np.diff(off)
+    live = np.nonzero(deg)[0]
+    remap = np.full(len(deg), -1, np.int64)
+    remap[live] = np.arange(len(live))
+    off2 = np.zeros(len(live) + 1, np.int64)
+    off2[1:] = np.cumsum(deg[live])
+    return off2, remap[idx].astype(np.int32)
+
+
+def reference_gpu_extra(names, timeout=900):
+    """The reference's own GPU solvers on the other workloads (opt-in, one
+    JSON line): k-cliques (CFSolver through oracle/ref_cf_driver.cu, whole
+    call timed) on R-MAT scale 20, edge factor 16, seed 1, and 4-vertex
+    motifs (G2MinerSolver / PatternSolver "Motif4", their own kernel-window
+    lines, src/G2MinerSolver.cuh:110-163, src/PatternSolver.cuh:177-248) on
+    R-MAT scale 18, edge factor 16, seed 1."""
+    import re
+    import tempfile
+    import gpm
+    import _oracle as orc
+    ref = os.path.join(ROOT, "oracle", "_ref")
+
+    def run(argv):
+        try:
+            return subprocess.run(argv, capture_output=True, text=True, timeout=timeout).stdout
+        except subprocess.TimeoutExpired:
+            return ""
+
+    res = {"impl": "reference", "extra": True}
+    with tempfile.TemporaryDirectory() as td:
+        if "clique" in names:
+            n, s_, d_ = gpm.gen_rmat(20, EF, A, B, C, seed=1)
+            off, idx = _compact_csr(*orc.build_csr(n, s_, d_))
+            mtx = os.path.join(td, "r20.mtx")
+            orc.write_mtx(mtx, off, idx)
+            for k in (4, 5):
+                out = run([os.path.join(ref, "ref_cf"), mtx, str(k)])
+                c = re.findall(r"Result: (\d+)", out)
+                t = re.findall(r"CFSolver call time: ([0-9.eE+-]+) seconds", out)
+                res[f"clique{k}_rmat20"] = ({"cliques": int(c[-1]), "s_call": float(t[-1])} if c and t
+                                            else {"unavailable": "no result"})
+        if "motif" in names:
+            n, s_, d_ = gpm.gen_rmat(18, EF, A, B, C, seed=1)
+            off, idx = _compact_csr(*orc.build_csr(n, s_, d_))
+            mtx = os.path.join(td, "r18.mtx")
+            orc.write_mtx(mtx, off, idx)
+            for fam, drv in (("g2miner", "test_G2Miner"), ("pattern_solver", "test_patternEnum")):
+                out = run([os.path.join(ref, drv), mtx, "Motif4"])
+                t = re.findall(r"matching\s+time:\s*([0-9.eE+-]+)\s*seconds", out)
+                got = dict(re.findall(r"Result(\d): (\d+)", out))
+                res[f"motif4_rmat18_{fam}"] = ({"s_kernel": float(t[-1]),
+                                                "counts": [int(got[str(i)]) for i in range(6)]}
+                                               if t and len(got) == 6 else {"unavailable": "no result"})
     return res
 
 
@@ -421,6 +477,8 @@ def reference_arm(args, rank, world, dist):
     if not args.no_ref_gpu:
         line["reference_gpu"] = reference_gpu(off, idx, m_und)
     print(json.dumps(line), flush=True)
+    if args.ref_extra:
+        print(json.dumps(reference_gpu_extra(args.ref_extra.split(","))), flush=True)
     if dist:
         dist.destroy_process_group()
 
