@@ -161,15 +161,19 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
 
 // ------------------------------------------------------------ features
 // Owner x (a task of the heuristic plan): 8 features from its key list and
-// its partner segments.  One warp per owner; lane 0 writes.
+// its partner segments (the front plong[x] and back pshort[x] slots of its
+// room).  One warp per owner; lane 0 writes.
 __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restrict__ roff,
                                                const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                                               const longlong2 *__restrict__ pseg, unsigned lane, float *f) {
+                                               const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
+                                               const int32_t *__restrict__ pshort, unsigned lane, float *f) {
   const int64_t d = roff[x + 1] - roff[x];
+  const int nl = plong[x], nseg = nl + pshort[x];
+  const int64_t back = poff[x + 1] - pshort[x] - nl;  // slot i >= nl lives at back + i
   unsigned long long work = 0;
   long long mx = 0, nlong = 0;
-  for (int64_t j = poff[x] + lane; j < poff[x + 1]; j += 32) {
-    const longlong2 sg = pseg[j];
+  for (int i = (int)lane; i < nseg; i += 32) {
+    const longlong2 sg = pseg[i < nl ? poff[x] + i : back + i];
     long long len = sg.y - sg.x;
     work += (unsigned long long)len;
     mx = max(mx, len);
@@ -180,7 +184,7 @@ __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restr
   for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   const long long span = d > 0 ? (long long)radj[roff[x + 1] - 1] - radj[roff[x]] + 1 : 0;
   f[0] = log2f(1.f + (float)d);
-  f[1] = log2f(1.f + (float)(poff[x + 1] - poff[x]));
+  f[1] = log2f(1.f + (float)nseg);
   f[2] = log2f(1.f + (float)work);
   f[3] = log2f(1.f + (float)mx);
   f[4] = log2f(1.f + (float)nlong);
@@ -191,13 +195,14 @@ __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restr
 
 __global__ void k_features(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
                            const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                           const longlong2 *__restrict__ pseg, float *__restrict__ X) {
+                           const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
+                           const int32_t *__restrict__ pshort, float *__restrict__ X) {
   const unsigned lane = lane_id();
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t t = warp; t < ntasks; t += nw) {
     float f[kIn];
-    owner_features(tasks[t], roff, radj, poff, pseg, lane, f);
+    owner_features(tasks[t], roff, radj, poff, pseg, plong, pshort, lane, f);
     if (lane == 0)
       for (int i = 0; i < kIn; ++i) X[t * kIn + i] = f[i];
   }
@@ -217,6 +222,7 @@ __global__ void k_gather_costs(const int32_t *__restrict__ tasks, int ntasks, co
 __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ tasks, int ntasks,
                                                 const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
                                                 const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
+                                                const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
                                                 const float *__restrict__ w, uint8_t *__restrict__ cfg,
                                                 float *__restrict__ warp_cost, uint8_t *__restrict__ cta_alt,
                                                 double *__restrict__ total) {
@@ -230,7 +236,7 @@ __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ task
   for (int64_t t = warp; t < ntasks; t += nw) {
     float f[kIn];
     const int32_t x = tasks[t];
-    owner_features(x, roff, radj, poff, pseg, lane, f);
+    owner_features(x, roff, radj, poff, pseg, plong, pshort, lane, f);
     if (lane == 0) {
       float h1[kH], h2[kH], y[kOut];
       mlp_forward(sw, f, h1, h2, y);
@@ -296,7 +302,8 @@ static int assign_configs(gpm_graph *g, gpm_sched *s, const int32_t *tasks, int 
   GPM_CUDA(cudaMemsetAsync(total.p, 0, sizeof(double), st));
   RankPlan *h = g->rank;
   k_assign<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p, h->pseg.p,
-                                                     s->w.p, cfg, warp_cost.p, cta_alt.p, total.p);
+                                                     h->plong.p, h->pshort.p, s->w.p, cfg, warp_cost.p, cta_alt.p,
+                                                     total.p);
   GPM_LAUNCH_CHECK();
   // warp slots of the count kernel: 8 CTAs of 8 warps per SM
   k_rail<<<blocks(nt), 256, 0, st>>>(tasks, nt, warp_cost.p, cta_alt.p, total.p, 64.0 * num_sms(), cfg);
@@ -429,7 +436,7 @@ int gpm_sched_collect(gpm_sched *s, gpm_graph *g, int64_t *rows_added) {
   }
   RankPlan *h = g->rank;
   k_features<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p,
-                                                       h->pseg.p, s->X.p + s->rows * kIn);
+                                                       h->pseg.p, h->plong.p, h->pshort.p, s->X.p + s->rows * kIn);
   DevBuf<unsigned long long> rec, cnt;
   DevBuf<uint8_t> cfg;
   GPM_TRY(rec.reserve(g->n));

@@ -431,13 +431,14 @@ int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, i
   GPM_TRY(g.off.reserve(n + 1));
   GPM_TRY(g.adj.reserve(nnz));
   GPM_CUDA(cudaMemcpyAsync(g.off.p, offsets, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st));
-  if (nnz > 0) GPM_CUDA(cudaMemcpyAsync(g.adj.p, indices, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
   if (variant == GPM_TC_AUTO) variant = GPM_TC_BITMAP;
   if (variant == GPM_TC_BITMAP || variant == GPM_TC_LEARNED) {
-    // orientation folded into the rank relabel (one pass instead of two)
-    GPM_TRY(ensure_rank_graph(&g, st, nullptr, 1, true));
+    // orientation folded into the rank relabel, the adjacency uploaded in
+    // chunks that are relabelled as they land
+    GPM_TRY(build_upward_rank_graph(&g, st, offsets, indices));
     g.oriented = 1;
   } else {
+    if (nnz > 0) GPM_CUDA(cudaMemcpyAsync(g.adj.p, indices, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
     GPM_TRY(orient_on_stream(&g, st));
   }
   GPM_TRY(g.result.reserve(8));

@@ -30,6 +30,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 #include "tc.cuh"
@@ -83,23 +84,22 @@ struct HashTable {
   }
 };
 
-// Segments [p0, p1) of one owner.  The first nlong are long: each half-warp
-// streams one, 16 keys per step (each step one coalesced 64-byte row), so
-// the per-segment work of a warp is shared by two segments; the rest are
-// short: 8-lane groups, four segments per warp.  `wid`/`nw` spread segments
+// Segments of one owner: the long ones [l0, l1): each half-warp streams one,
+// 16 keys per step (each step one coalesced 64-byte row), so the
+// per-segment work of a warp is shared by two segments; the short ones
+// [s0, s1): 8-lane groups, four segments per warp.  `wid`/`nw` spread segments
 // over the warps of the executing group (1 warp for warp tasks, the CTA's
 // warps for CTA tasks).  R-MAT 22: half-warps 7.0 ms against 7.6 ms for
 // whole-warp streaming of the same segments.
 template <class T>
 __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__restrict__ radj,
-                                                            const longlong2 *__restrict__ pseg, int64_t p0,
-                                                            int64_t p1, int nlong, const T &t, int wid, int nw,
-                                                            unsigned lane) {
+                                                            const longlong2 *__restrict__ pseg, int64_t l0,
+                                                            int64_t l1, int64_t s0, int64_t s1, const T &t,
+                                                            int wid, int nw, unsigned lane) {
   unsigned long long c = 0;
-  const int64_t pl = p0 + nlong;
   const unsigned half = lane >> 4, hl = lane & 15;
   int64_t j;
-  for (j = p0 + wid * 2 + half; j < pl; j += nw * 2) {
+  for (j = l0 + wid * 2 + half; j < l1; j += nw * 2) {
     const longlong2 sg = pseg[j];
     const int32_t *__restrict__ q = radj + sg.x;
     const int len = (int)(sg.y - sg.x);
@@ -109,7 +109,7 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
     c += cs;
   }
   const unsigned grp = lane >> 3, gl = lane & 7;
-  for (j = pl + wid * 4 + grp; j < p1; j += nw * 4) {
+  for (j = s0 + wid * 4 + grp; j < s1; j += nw * 4) {
     const longlong2 sg = pseg[j];
     unsigned cs = 0;
     for (int64_t k = sg.x + gl; k < sg.y; k += 8) cs += t.hit(__ldg(radj + k));
@@ -140,7 +140,8 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
                                                          const int32_t *__restrict__ radj,
                                                          const int64_t *__restrict__ poff,
                                                          const longlong2 *__restrict__ pseg,
-                                                         const int32_t *__restrict__ plong, uint32_t *words,
+                                                         const int32_t *__restrict__ plong,
+                                                         const int32_t *__restrict__ pshort, uint32_t *words,
                                                          int nwords, unsigned long long *rec) {
   const long long t0 = REC ? clock64() : 0;
   const int tid = CTA ? (int)threadIdx.x : (int)lane_id(), nthr = CTA ? (int)blockDim.x : 32;
@@ -148,8 +149,7 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
   const unsigned lane = lane_id();
   const int64_t s0 = roff[x];
   const int d = (int)(roff[x + 1] - s0);
-  const int64_t p0 = poff[x], p1 = poff[x + 1];
-  const int nl = plong[x];
+  const int64_t l0 = poff[x], l1 = l0 + plong[x], h1 = poff[x + 1], h0 = h1 - pshort[x];
   const int32_t kmin = radj[s0], kmax = radj[s0 + d - 1];
   const int64_t span = (int64_t)kmax - kmin + 1;
   unsigned long long c = 0;
@@ -160,7 +160,7 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
     uint8_t *bytes = reinterpret_cast<uint8_t *>(words);
     for (int i = tid; i < d; i += nthr) bytes[radj[s0 + i] - kmin] = 1;
     group_sync<CTA>();
-    c = scan_segments(radj, pseg, p0, p1, nl, ByteTable{bytes, kmin}, wid, nw, lane);
+    c = scan_segments(radj, pseg, l0, l1, h0, h1, ByteTable{bytes, kmin}, wid, nw, lane);
   } else if (span <= (int64_t)nwords * 32) {
     const int nclear = (int)((span + 31) >> 5);
     for (int i = tid; i < nclear; i += nthr) words[i] = 0u;
@@ -170,7 +170,7 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
       atomicOr(&words[o >> 5], 1u << (o & 31));
     }
     group_sync<CTA>();
-    c = scan_segments(radj, pseg, p0, p1, nl, BitTable{words, kmin}, wid, nw, lane);
+    c = scan_segments(radj, pseg, l0, l1, h0, h1, BitTable{words, kmin}, wid, nw, lane);
   } else {
     int32_t *tab = reinterpret_cast<int32_t *>(words);
     const int logcap = 31 - __clz(nwords);
@@ -187,7 +187,7 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
         while (atomicCAS(&tab[h], -1, key) != -1) h = (h + 1) & mask;
       }
       group_sync<CTA>();
-      c += scan_segments(radj, pseg, p0, p1, nl, HashTable{tab, logcap}, wid, nw, lane);
+      c += scan_segments(radj, pseg, l0, l1, h0, h1, HashTable{tab, logcap}, wid, nw, lane);
     }
   }
   if (REC && lane == 0) atomicAdd(rec, (unsigned long long)(clock64() - t0));
@@ -208,7 +208,8 @@ template <bool REC>
 __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     k_tc_rank_t(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
                 const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
-                const int32_t *__restrict__ plong, const int32_t *__restrict__ cta_tasks, int n_cta,
+                const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
+                const int32_t *__restrict__ cta_tasks, int n_cta,
                 const int32_t *__restrict__ warp_tasks, int n_warp, int *__restrict__ counters,
                 unsigned long long *__restrict__ out, unsigned long long *__restrict__ rec) {
   extern __shared__ __align__(16) uint32_t rsm[];
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     __syncthreads();
     if (t >= n_cta) break;
     const int32_t x = cta_tasks[t];
-    c += owner_task<true, REC>(x, roff, radj, poff, pseg, plong, rsm, kCtaWords, REC ? rec + x : nullptr);
+    c += owner_task<true, REC>(x, roff, radj, poff, pseg, plong, pshort, rsm, kCtaWords, REC ? rec + x : nullptr);
   }
   const int wid = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31;
@@ -232,7 +233,7 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= n_warp) break;
     const int32_t x = warp_tasks[t];
-    c += owner_task<false, REC>(x, roff, radj, poff, pseg, plong, region, kWarpWords, REC ? rec + x : nullptr);
+    c += owner_task<false, REC>(x, roff, radj, poff, pseg, plong, pshort, region, kWarpWords, REC ? rec + x : nullptr);
   }
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(out, c);
@@ -263,12 +264,11 @@ __global__ void k_rank_inverse(int64_t n, const int32_t *__restrict__ order, con
   }
 }
 // Relabelled lists, gathered and sorted in one pass (one warp per rank r):
-// the neighbours of order[r] as ranks (UPWARD: only ranks above r, the
-// degree-oriented DAG of a symmetric graph, graph.h:128-129) are compacted
-// into the warp's shared buffer, sorted there -- a register bitonic network
-// up to 32 keys, a shared-memory one up to kSortCap -- and written to
-// out[roff[r] ..].  Longer lists are written unsorted and their rank
-// appended to big[] for a segmented sort afterwards.
+// the neighbours of order[r] as ranks are collected in the warp's shared
+// buffer, sorted there -- a register bitonic network up to 32 keys, a
+// shared-memory one up to kSortCap -- and written to out[roff[r] ..].
+// Longer lists are written unsorted and their rank appended to big[] for a
+// segmented sort afterwards.
 constexpr int kSortCap = 1024;
 constexpr int kGatherWarps = 8;
 
@@ -284,7 +284,6 @@ __device__ __forceinline__ int32_t warp_bitonic32(int32_t key, unsigned lane) {
   return key;
 }
 
-template <bool UPWARD>
 __global__ void __launch_bounds__(kGatherWarps * 32)
     k_rank_gather_sort(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ rank,
                        const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
@@ -306,7 +305,7 @@ __global__ void __launch_bounds__(kGatherWarps * 32)
     for (int64_t base = s; base < e && filled < len; base += 32) {
       const int64_t k = base + lane;
       const int32_t x = k < e ? rank[adj[k]] : -1;
-      const bool keep = k < e && (!UPWARD || x > (int32_t)r);
+      const bool keep = k < e;
       const unsigned m = __ballot_sync(0xffffffffu, keep);
       if (keep) dst[filled + __popc(m & ((1u << lane) - 1u))] = x;
       filled += __popc(m);
@@ -344,6 +343,13 @@ __global__ void __launch_bounds__(kGatherWarps * 32)
   }
 }
 
+// incident edges of rank r: its out-degree plus the in-degree of order[r]
+__global__ void k_incident(int64_t n, const int32_t *__restrict__ order, const int64_t *__restrict__ rdeg,
+                           const int32_t *__restrict__ indeg, int64_t *__restrict__ inc) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    inc[r] = rdeg[r] + indeg[order[r]];
+}
+
 __global__ void k_big_bounds(int nbig, const int32_t *__restrict__ big, const int64_t *__restrict__ roff,
                              int64_t *__restrict__ bb, int64_t *__restrict__ be) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbig; i += gridDim.x * blockDim.x) {
@@ -357,21 +363,6 @@ __global__ void k_big_copy(int nbig, const int64_t *__restrict__ bb, const int64
     for (int64_t k = bb[i] + threadIdx.x; k < be[i]; k += blockDim.x) dst[k] = src[k];
 }
 
-// Orientation folded into the relabel: keep only neighbours of larger rank
-// (the degree-oriented DAG of a symmetric graph, graph.h:128-129).
-__global__ void k_rank_up_count(int64_t n, const int32_t *__restrict__ order, const int32_t *__restrict__ rank,
-                                const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
-                                int64_t *__restrict__ rdeg) {
-  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t r = warp; r < n; r += nw) {
-    int32_t v = order[r];
-    int64_t c = 0;
-    for (int64_t k = off[v] + lane_id(); k < off[v + 1]; k += 32) c += rank[adj[k]] > (int32_t)r;
-    c = warp_sum(c);
-    if (lane_id() == 0) rdeg[r] = c;
-  }
-}
 // Per-owner task configuration (learned scheduler): queue = cfg / 3
 // (0 warp, 1 CTA), long-segment threshold = kCfgLong[cfg % 3].
 __device__ __constant__ int kCfgLong[3] = {16, 64, 256};
@@ -402,20 +393,23 @@ __device__ __forceinline__ int64_t upper_bound_key(const int32_t *__restrict__ a
   return lo;
 }
 
-// Stored edge k = (u, radj[k]): the endpoint with the longer list owns it
-// (ties to u), the other is its partner.  The segment is the part of the
-// partner's list inside [min, max] of the owner's list; its start and length
-// go to sstart[k] / slen[k] (length 0: nothing to stream, also when the
-// owner has fewer than 2 keys and so closes no triangle through the edge).
-// upward: every list holds only ids above its vertex, so when u owns the
-// edge, min N(u) <= v < every id of N(v) and the lower search is skipped.
-// Per-owner counters take one atomic per (owner, class) and warp, the lanes
-// of a warp that share them combined first (hub owners get most of theirs
-// from their own list, i.e. from one warp).
-__global__ void k_partner_count(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+// Every stored edge k = (u, radj[k]) placed in one pass: the endpoint with
+// the longer list owns it (ties to u), the other is its partner; the segment
+// is the part of the partner's list inside [min, max] of the owner's list
+// (empty, hence left out, also when the owner has fewer than 2 keys and so
+// closes no triangle through the edge).  It goes into the owner's room
+// [poff[x], poff[x+1]) -- one slot per incident edge, so it always fits --
+// long segments from the front (cursor plong[x]), short ones from the back
+// (cursor pshort[x]).  upward: every list holds only ids above its vertex,
+// so when u owns the edge, min N(u) <= v < every id of N(v) and the lower
+// search is skipped.  The lanes of a warp that share an (owner, class) take
+// their slots with one atomic (hub owners get most of theirs from their own
+// list, i.e. from one warp).
+__global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
                                 int upward, int long_min, const uint8_t *__restrict__ cfg,
-                                int32_t *__restrict__ nlong, int32_t *__restrict__ nshort,
-                                int64_t *__restrict__ sstart, int32_t *__restrict__ slen) {
+                                const int64_t *__restrict__ poff, int32_t *__restrict__ plong,
+                                int32_t *__restrict__ pshort, longlong2 *__restrict__ pseg,
+                                unsigned long long *__restrict__ work) {
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = warp; u < n; u += nw) {
@@ -427,55 +421,17 @@ __global__ void k_partner_count(int64_t n, const int64_t *__restrict__ roff, con
       int32_t owner = own_u ? (int32_t)u : v;
       int64_t os = own_u ? s : vs, oe = own_u ? e : ve;
       int64_t ps = own_u ? vs : s, pe = own_u ? ve : e;
-      int64_t lo = 0, len = 0;
-      if (oe - os >= 2) {
-        lo = upward && own_u ? ps : lower_bound_key(radj, ps, pe, radj[os]);
-        len = upper_bound_key(radj, lo, pe, radj[oe - 1]) - lo;
-      }
-      sstart[k] = lo;
-      slen[k] = (int32_t)len;
-      if (len > 0) {
-        const bool lng = len >= owner_long_min(cfg, owner, long_min);
-        cg::coalesced_group grp =
-            cg::labeled_partition(cg::coalesced_threads(), ((unsigned long long)(uint32_t)owner << 1) | lng);
-        if (grp.thread_rank() == 0) atomicAdd(lng ? &nlong[owner] : &nshort[owner], (int)grp.size());
-      }
-    }
-  }
-}
-__global__ void k_partner_sizes(int64_t n, const int32_t *__restrict__ nlong, const int32_t *__restrict__ nshort,
-                                int64_t *__restrict__ tot) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    tot[i] = (int64_t)nlong[i] + nshort[i];
-}
-__global__ void k_partner_cursors(int64_t n, const int64_t *__restrict__ poff, const int32_t *__restrict__ nlong,
-                                  unsigned long long *__restrict__ curl, unsigned long long *__restrict__ curs) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    curl[i] = (unsigned long long)poff[i];
-    curs[i] = (unsigned long long)(poff[i] + nlong[i]);
-  }
-}
-__global__ void k_partner_fill(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                               int long_min, const uint8_t *__restrict__ cfg, const int64_t *__restrict__ sstart,
-                               const int32_t *__restrict__ slen, unsigned long long *__restrict__ curl,
-                               unsigned long long *__restrict__ curs, longlong2 *__restrict__ pseg,
-                               unsigned long long *__restrict__ work) {
-  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t u = warp; u < n; u += nw) {
-    int64_t s = roff[u], e = roff[u + 1], du = e - s;
-    for (int64_t k = s + lane_id(); k < e; k += 32) {
-      const int32_t len = slen[k];
+      if (oe - os < 2) continue;
+      const int64_t lo = upward && own_u ? ps : lower_bound_key(radj, ps, pe, radj[os]);
+      const int64_t len = upper_bound_key(radj, lo, pe, radj[oe - 1]) - lo;
       if (len == 0) continue;
-      int32_t v = radj[k];
-      int32_t owner = roff[v + 1] - roff[v] <= du ? (int32_t)u : v;
       const bool lng = len >= owner_long_min(cfg, owner, long_min);
       cg::coalesced_group grp =
           cg::labeled_partition(cg::coalesced_threads(), ((unsigned long long)(uint32_t)owner << 1) | lng);
-      unsigned long long pos = 0;
-      if (grp.thread_rank() == 0) pos = atomicAdd(lng ? &curl[owner] : &curs[owner], (unsigned long long)grp.size());
-      pos = grp.shfl(pos, 0) + grp.thread_rank();
-      const int64_t lo = sstart[k];
+      int base = 0;
+      if (grp.thread_rank() == 0) base = atomicAdd(lng ? &plong[owner] : &pshort[owner], (int)grp.size());
+      const int64_t slot = grp.shfl(base, 0) + (int64_t)grp.thread_rank();
+      const int64_t pos = lng ? poff[owner] + slot : poff[owner + 1] - 1 - slot;
       pseg[pos] = make_longlong2(lo, lo + len);
       const unsigned long long w = cg::reduce(grp, (unsigned long long)len + 1ull, cg::plus<unsigned long long>());
       if (grp.thread_rank() == 0) atomicAdd(&work[owner], w);
@@ -483,13 +439,14 @@ __global__ void k_partner_fill(int64_t n, const int64_t *__restrict__ roff, cons
   }
 }
 // tasks: owners with partners; key = ~work so an ascending sort puts heavy first
-__global__ void k_rank_tasks(int64_t n, const int64_t *__restrict__ roff, const int64_t *__restrict__ poff,
+__global__ void k_rank_tasks(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ plong,
+                             const int32_t *__restrict__ pshort,
                              const unsigned long long *__restrict__ work, int cta_min,
                              const uint8_t *__restrict__ cfg, unsigned long long *__restrict__ ckey,
                              int32_t *__restrict__ cval, unsigned long long *__restrict__ wkey,
                              int32_t *__restrict__ wval, int *__restrict__ sizes) {
   for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
-    if (poff[x + 1] == poff[x]) continue;
+    if (plong[x] + pshort[x] == 0) continue;
     int64_t d = roff[x + 1] - roff[x];
     if (cfg ? cfg[x] / 3 == 1 : d > cta_min) {
       int i = atomicAdd(&sizes[0], 1);
@@ -540,89 +497,333 @@ void free_rank_graph(RankGraph *r) { delete r; }
 // With a per-vertex graph id (a disjoint union of graphs whose vertices are
 // contiguous id ranges) the key is (graph id, degree), so every member graph
 // keeps its id range and is ranked within itself.
+// Lists of the ranks in big[0..nbig) sorted in place by a segmented sort,
+// then r->upward set by checking every list against its rank.
+static int finish_rank_graph(RankGraph *r, int64_t n, int64_t nnz, const int32_t *big, int hbig, cudaStream_t st) {
+  int s;
+  if (hbig > 0) {
+    DevBuf<int64_t> bb, be;
+    DevBuf<int32_t> sorted;
+    if ((s = bb.reserve(hbig)) || (s = be.reserve(hbig)) || (s = sorted.reserve(nnz))) return s;
+    k_big_bounds<<<grid_for(hbig), 256, 0, st>>>(hbig, big, r->roff.p, bb.p, be.p);
+    size_t tmp = 0;
+    GPM_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, r->radj.p, sorted.p, (int)nnz, hbig, bb.p, be.p, st));
+    DevBuf<char> t;
+    if ((s = t.reserve(tmp))) return s;
+    GPM_CUDA(cub::DeviceSegmentedSort::SortKeys(t.p, tmp, r->radj.p, sorted.p, (int)nnz, hbig, bb.p, be.p, st));
+    k_big_copy<<<std::min(hbig, num_sms() * 8), 256, 0, st>>>(hbig, bb.p, be.p, sorted.p, r->radj.p);
+  }
+  // does every stored edge point to a larger rank? (true for a degree-oriented DAG)
+  DevBuf<int> down;
+  if ((s = down.reserve(1))) return s;
+  cudaMemsetAsync(down.p, 0, sizeof(int), st);
+  k_count_down<<<grid_for(n), 256, 0, st>>>(n, r->roff.p, r->radj.p, down.p);
+  int hdown = 0;
+  cudaMemcpyAsync(&hdown, down.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(GPM_ECUDA, std::string("rank relabel: ") + cudaGetErrorString(e));
+  r->upward = hdown == 0;
+  return GPM_OK;
+}
+
+// Rank keys of the stored graph sorted: order[rank] = vertex, rank[vertex].
+// indeg == nullptr: a symmetric graph (out-degree orders like in + out).
+static int rank_order(gpm_graph *g, const int32_t *indeg, const int32_t *gid, int ngraphs, int32_t *order,
+                      int32_t *rank, int64_t *rdeg, cudaStream_t st) {
+  const int64_t n = g->n;
+  int s;
+  DevBuf<int32_t> val;
+  DevBuf<uint64_t> key, key2;
+  if ((s = val.reserve(n)) || (s = key.reserve(n)) || (s = key2.reserve(n))) return s;
+  int end_bit = 32;
+  if (gid)
+    while (end_bit < 64 && (1ll << (end_bit - 32)) < ngraphs) ++end_bit;
+  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, indeg, gid, key.p, val.p);
+  size_t tmp = 0;
+  GPM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, val.p, order, (int)n, 0, end_bit, st));
+  DevBuf<char> t;
+  if ((s = t.reserve(tmp))) return s;
+  GPM_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key2.p, val.p, order, (int)n, 0, end_bit, st));
+  k_rank_inverse<<<grid_for(n), 256, 0, st>>>(n, order, g->off.p, rank, rdeg);
+  return GPM_OK;
+}
+
+// dst[0 .. len) sorted in place by one warp (len <= kSortCap): a register
+// bitonic network up to 32 ids, else a shared-memory network in buf.
+__device__ __forceinline__ void warp_sort_list(int32_t *dst, int64_t len, int32_t *buf, unsigned lane) {
+  if (len <= 1) return;
+  if (len <= 32) {
+    const int32_t key = warp_bitonic32((int64_t)lane < len ? dst[lane] : INT_MAX, lane);
+    if ((int64_t)lane < len) dst[lane] = key;
+    return;
+  }
+  int p = 64;
+  while (p < len) p <<= 1;
+  for (int i = lane; i < p; i += 32) buf[i] = i < len ? dst[i] : INT_MAX;
+  __syncwarp();
+  for (int k = 2; k <= p; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < p; i += 32) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const int32_t a = buf[i], b = buf[ixj];
+          if ((a > b) == ((i & k) == 0)) {
+            buf[i] = b;
+            buf[ixj] = a;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  for (int64_t i = lane; i < len; i += 32) dst[i] = buf[i];
+  __syncwarp();
+}
+
+// Upward lists of a symmetric graph, gathered chunk by chunk: for source
+// vertex v, the ranks of its neighbours above rank[v], appended (unsorted)
+// into tmp at v's own symmetric offset -- room for all of v's neighbours, so
+// no count pass is needed first.  A vertex with at most kHubBlock neighbours
+// is one warp's task; a longer list is cut into kHubBlock-entry block tasks
+// (queued here, run by k_up_gather_hub) so that no warp scans a hub's whole
+// list alone.
+constexpr int kHubBlock = 1024;
+static_assert(kHubBlock <= kSortCap, "a non-hub list must fit the sort buffer");
+
+__device__ __forceinline__ int64_t gather_upward(int32_t r, int64_t s, int64_t e, const int32_t *__restrict__ rank,
+                                                 const int32_t *__restrict__ adj, int32_t *dst,
+                                                 unsigned long long *cursor, unsigned lane) {
+  int64_t len = 0;
+  for (int64_t base = s; base < e; base += 32) {
+    const int64_t k = base + lane;
+    const int32_t x = k < e ? rank[adj[k]] : -1;
+    const bool keep = k < e && x > r;
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (m == 0) continue;
+    int64_t at = len;
+    if (cursor) {  // shared with the hub's other block tasks
+      unsigned long long b = 0;
+      if (lane == 0) b = atomicAdd(cursor, (unsigned long long)__popc(m));
+      at = (int64_t)__shfl_sync(0xffffffffu, b, 0);
+    }
+    if (keep) dst[at + __popc(m & ((1u << lane) - 1u))] = x;
+    len += __popc(m);
+  }
+  return len;
+}
+
+__global__ void __launch_bounds__(kGatherWarps * 32)
+    k_up_gather(int64_t v0, int64_t v1, const int32_t *__restrict__ rank, const int64_t *__restrict__ off,
+                const int32_t *__restrict__ adj, int32_t *__restrict__ tmp, int64_t *__restrict__ kept,
+                unsigned long long *__restrict__ hubcnt, int2 *__restrict__ hubq, int *__restrict__ nhubq) {
+  __shared__ int32_t sbuf[kGatherWarps][kSortCap];
+  int32_t *buf = sbuf[threadIdx.x >> 5];
+  const unsigned lane = lane_id();
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = v0 + warp; v < v1; v += nw) {
+    const int64_t s = off[v], e = off[v + 1];
+    if (e - s > kHubBlock) {
+      const int nb = (int)((e - s + kHubBlock - 1) / kHubBlock);
+      if (lane == 0) {
+        hubcnt[v] = 0;
+        const int at = atomicAdd(nhubq, nb);
+        for (int b = 0; b < nb; ++b) hubq[at + b] = make_int2((int)v, b);
+      }
+      continue;
+    }
+    const int32_t r = rank[v];
+    const int64_t len = gather_upward(r, s, e, rank, adj, tmp + s, nullptr, lane);
+    if (lane == 0) kept[r] = len;
+    __syncwarp();
+    warp_sort_list(tmp + s, len, buf, lane);  // len <= kHubBlock = kSortCap
+  }
+}
+
+__global__ void k_up_gather_hub(const int2 *__restrict__ hubq, const int *__restrict__ nhubq,
+                                const int32_t *__restrict__ rank, const int64_t *__restrict__ off,
+                                const int32_t *__restrict__ adj, int32_t *__restrict__ tmp,
+                                unsigned long long *__restrict__ hubcnt) {
+  const unsigned lane = lane_id();
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int nt = *nhubq;
+  for (int64_t t = warp; t < nt; t += nw) {
+    const int2 task = hubq[t];
+    const int64_t s = off[task.x], e = off[task.x + 1];
+    const int64_t b0 = s + (int64_t)task.y * kHubBlock, b1 = min(e, b0 + kHubBlock);
+    gather_upward(rank[task.x], b0, b1, rank, adj, tmp + s, &hubcnt[task.x], lane);
+  }
+}
+
+// kept[rank[v]] of the hubs queued at [q0, nhubq) (one entry per hub: b = 0)
+__global__ void k_up_hub_kept(const int2 *__restrict__ hubq, int q0, const int *__restrict__ nhubq,
+                              const int32_t *__restrict__ rank, const unsigned long long *__restrict__ hubcnt,
+                              int64_t *__restrict__ kept) {
+  const int nt = *nhubq;
+  for (int64_t t = q0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nt; t += (int64_t)gridDim.x * blockDim.x)
+    if (hubq[t].y == 0) kept[rank[hubq[t].x]] = (int64_t)hubcnt[hubq[t].x];
+}
+
+// radj[roff[r] ..] = tmp[off[order[r]] ..], one warp per rank.  Lists of
+// small vertices arrive sorted; a hub's list (assembled by block tasks) is
+// sorted here, or, beyond kSortCap ids, copied and its rank appended to big[].
+__global__ void __launch_bounds__(kGatherWarps * 32)
+    k_up_compact(int64_t n, const int32_t *__restrict__ order, const int64_t *__restrict__ off,
+                 int32_t *__restrict__ tmp, const int64_t *__restrict__ roff, int32_t *__restrict__ radj,
+                 int32_t *__restrict__ big, int *__restrict__ nbig) {
+  __shared__ int32_t sbuf[kGatherWarps][kSortCap];
+  int32_t *buf = sbuf[threadIdx.x >> 5];
+  const unsigned lane = lane_id();
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < n; r += nw) {
+    const int32_t v = order[r];
+    int32_t *src = tmp + off[v];
+    const int64_t o = roff[r], len = roff[r + 1] - o;
+    if (off[v + 1] - off[v] > kHubBlock) {
+      if (len > kSortCap) {
+        if (lane == 0) big[atomicAdd(nbig, 1)] = (int32_t)r;
+      } else {
+        warp_sort_list(src, len, buf, lane);
+      }
+    }
+    for (int64_t i = lane; i < len; i += 32) radj[o + i] = src[i];
+  }
+}
+
+int build_upward_rank_graph(gpm_graph *g, cudaStream_t st, const int64_t *h_off, const int32_t *h_adj) {
+  if (g->rg) return GPM_OK;
+  const int64_t n = g->n, nsym = g->nnz;
+  RankGraph *r = new RankGraph();
+  cudaStream_t cs = nullptr;
+  std::vector<cudaEvent_t> evs;
+  auto bail = [&](int s) {
+    if (cs) {
+      cudaStreamSynchronize(cs);
+      cudaStreamDestroy(cs);
+    }
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    delete r;
+    return s;
+  };
+  int s;
+  DevBuf<int32_t> rank, tmp, big;
+  DevBuf<int64_t> kept, inc;
+  DevBuf<int> nbig, nhubq;
+  DevBuf<unsigned long long> hubcnt;
+  DevBuf<int2> hubq;
+  // hub block tasks: at most nsym / kHubBlock + (number of hubs) of them
+  const int64_t maxq = nsym / kHubBlock + nsym / (kHubBlock + 1) + 1;
+  if ((s = r->order.reserve(n)) || (s = rank.reserve(n)) || (s = kept.reserve(n)) || (s = r->roff.reserve(n + 1)) ||
+      (s = inc.reserve(n)) || (s = r->rinc.reserve(n + 1)) || (s = tmp.reserve(std::max<int64_t>(nsym, 1))) ||
+      (s = big.reserve(n)) || (s = nbig.reserve(1)) ||
+      (s = nhubq.reserve(1)) || (s = hubcnt.reserve(n)) || (s = hubq.reserve(maxq)))
+    return bail(s);
+  // vertex ranges of the adjacency chunks (about nsym / 8 edges each)
+  std::vector<int64_t> cut{0};
+  if (h_adj && nsym > 0) {
+    const int chunks = 8;
+    for (int c = 1; c < chunks; ++c) {
+      const int64_t want = nsym * c / chunks;
+      int64_t v = std::lower_bound(h_off, h_off + n + 1, want) - h_off;
+      if (v > cut.back() && v < n) cut.push_back(v);
+    }
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+      cs = nullptr;
+      return bail(fail(GPM_ECUDA, "copy stream"));
+    }
+  }
+  cut.push_back(n);
+  // 1. the adjacency upload, chunk by chunk on its own stream
+  if (h_adj)
+    for (size_t c = 0; c + 1 < cut.size(); ++c) {
+      const int64_t e0 = h_off[cut[c]], e1 = h_off[cut[c + 1]];
+      cudaEvent_t ev;
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(GPM_ECUDA, "event"));
+      evs.push_back(ev);
+      if (e1 > e0 && cudaMemcpyAsync(g->adj.p + e0, h_adj + e0, sizeof(int32_t) * (e1 - e0),
+                                     cudaMemcpyHostToDevice, cs) != cudaSuccess)
+        return bail(fail(GPM_ECUDA, "adjacency upload"));
+      cudaEventRecord(ev, cs);
+    }
+  // 2. ranks from the degrees alone (symmetric input), meanwhile; a
+  // vertex's symmetric degree is its incident-edge count in the DAG
+  if ((s = rank_order(g, nullptr, nullptr, 1, r->order.p, rank.p, inc.p, st))) return bail(s);
+  if ((s = scan_i64(n, inc.p, r->rinc.p, st))) return bail(s);
+  // 3. each chunk gathered as soon as it has landed: small lists one warp
+  // each, hub lists as block tasks over the whole grid
+  cudaMemsetAsync(nbig.p, 0, sizeof(int), st);
+  cudaMemsetAsync(nhubq.p, 0, sizeof(int), st);
+  const int qgrid = num_sms() * 8;
+  for (size_t c = 0; c + 1 < cut.size(); ++c) {
+    if (h_adj) cudaStreamWaitEvent(st, evs[c], 0);
+    const int64_t nv = cut[c + 1] - cut[c];
+    if (nv == 0) continue;
+    // the queue is drained by this chunk's hub launch, so each chunk starts it at 0
+    cudaMemsetAsync(nhubq.p, 0, sizeof(int), st);
+    k_up_gather<<<grid_for(nv * 32), 256, 0, st>>>(cut[c], cut[c + 1], rank.p, g->off.p, g->adj.p, tmp.p, kept.p,
+                                                   hubcnt.p, hubq.p, nhubq.p);
+    k_up_gather_hub<<<qgrid, 256, 0, st>>>(hubq.p, nhubq.p, rank.p, g->off.p, g->adj.p, tmp.p, hubcnt.p);
+    k_up_hub_kept<<<qgrid, 256, 0, st>>>(hubq.p, 0, nhubq.p, rank.p, hubcnt.p, kept.p);
+  }
+  // 4. list offsets, then the lists moved to them
+  if ((s = scan_i64(n, kept.p, r->roff.p, st))) return bail(s);
+  int64_t nnz = 0;
+  int hbig = 0;
+  cudaMemcpyAsync(&nnz, r->roff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&r->nin, r->rinc.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank relabel: ") + cudaGetErrorString(e)));
+  if ((s = r->radj.reserve(std::max<int64_t>(nnz, 1)))) return bail(s);
+  k_up_compact<<<grid_for(n * 32, kGatherWarps * 32), kGatherWarps * 32, 0, st>>>(
+      n, r->order.p, g->off.p, tmp.p, r->roff.p, r->radj.p, big.p, nbig.p);
+  cudaMemcpyAsync(&hbig, nbig.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank relabel: ") + cudaGetErrorString(e)));
+  if ((s = finish_rank_graph(r, n, nnz, big.p, hbig, st))) return bail(s);
+  if (cs) cudaStreamDestroy(cs);
+  cs = nullptr;
+  for (cudaEvent_t ev : evs) cudaEventDestroy(ev);
+  evs.clear();
+  g->rg = r;
+  return GPM_OK;
+}
+
 int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid, int ngraphs, bool upward_only) {
   if (g->rg) return GPM_OK;
-  const int64_t n = g->n;
-  int64_t nnz = g->nnz;
+  if (upward_only) return build_upward_rank_graph(g, st, nullptr, nullptr);
+  const int64_t n = g->n, nnz = g->nnz;
   RankGraph *r = new RankGraph();
   auto bail = [&](int s) {
     delete r;
     return s;
   };
   int s;
-  DevBuf<int32_t> indeg, val, rank;
-  DevBuf<uint64_t> key, key2;
-  DevBuf<int64_t> rdeg;
-  DevBuf<int> down;
-  if ((s = indeg.reserve(n)) || (s = val.reserve(n)) || (s = r->order.reserve(n)) || (s = rank.reserve(n)) ||
-      (s = key.reserve(n)) || (s = key2.reserve(n)) || (s = rdeg.reserve(n)) || (s = r->roff.reserve(n + 1)) ||
-      (s = r->radj.reserve(nnz)) || (s = down.reserve(1)))
+  DevBuf<int32_t> indeg, rank, big;
+  DevBuf<int64_t> rdeg, inc;
+  DevBuf<int> nbig;
+  if ((s = indeg.reserve(n)) || (s = r->order.reserve(n)) || (s = rank.reserve(n)) || (s = rdeg.reserve(n)) ||
+      (s = inc.reserve(n)) || (s = r->roff.reserve(n + 1)) || (s = r->rinc.reserve(n + 1)) ||
+      (s = r->radj.reserve(std::max<int64_t>(nnz, 1))) || (s = big.reserve(n)) || (s = nbig.reserve(1)))
     return bail(s);
-  int32_t *order = r->order.p;
-  int end_bit = 32;
-  if (gid)
-    while (end_bit < 64 && (1ll << (end_bit - 32)) < ngraphs) ++end_bit;
-  // upward_only takes a symmetric graph, whose in-degrees equal its
-  // out-degrees: the key needs no in-degree pass then
-  if (!upward_only) {
-    cudaMemsetAsync(indeg.p, 0, sizeof(int32_t) * n, st);
-    k_indeg<<<grid_for(nnz), 256, 0, st>>>(nnz, g->adj.p, indeg.p);
-  }
-  k_rank_keys<<<grid_for(n), 256, 0, st>>>(n, g->off.p, upward_only ? nullptr : indeg.p, gid, key.p, val.p);
-  {
-    size_t tmp = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key2.p, val.p, order, (int)n, 0, end_bit, st);
-    DevBuf<char> t;
-    if ((s = t.reserve(tmp))) return bail(s);
-    cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key2.p, val.p, order, (int)n, 0, end_bit, st);
-  }
-  k_rank_inverse<<<grid_for(n), 256, 0, st>>>(n, order, g->off.p, rank.p, rdeg.p);
-  if (upward_only)
-    k_rank_up_count<<<grid_for(n * 32), 256, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, rdeg.p);
+  cudaMemsetAsync(indeg.p, 0, sizeof(int32_t) * n, st);
+  k_indeg<<<grid_for(nnz), 256, 0, st>>>(nnz, g->adj.p, indeg.p);
+  if ((s = rank_order(g, indeg.p, gid, ngraphs, r->order.p, rank.p, rdeg.p, st))) return bail(s);
   if ((s = scan_i64(n, rdeg.p, r->roff.p, st))) return bail(s);
-  if (upward_only) {
-    cudaMemcpyAsync(&nnz, r->roff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
-  }
-  {
-    // gather + sort in one pass; lists longer than kSortCap get a segmented
-    // sort of their own afterwards
-    DevBuf<int32_t> big;
-    DevBuf<int> nbig;
-    if ((s = big.reserve(n)) || (s = nbig.reserve(1))) return bail(s);
-    cudaMemsetAsync(nbig.p, 0, sizeof(int), st);
-    const int ggrid = grid_for(n * 32, kGatherWarps * 32);
-    if (upward_only)
-      k_rank_gather_sort<true><<<ggrid, kGatherWarps * 32, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p, r->roff.p,
-                                                                    r->radj.p, big.p, nbig.p);
-    else
-      k_rank_gather_sort<false><<<ggrid, kGatherWarps * 32, 0, st>>>(n, order, rank.p, g->off.p, g->adj.p,
-                                                                     r->roff.p, r->radj.p, big.p, nbig.p);
-    int hbig = 0;
-    cudaMemcpyAsync(&hbig, nbig.p, sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaError_t e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank relabel: ") + cudaGetErrorString(e)));
-    if (hbig > 0) {
-      DevBuf<int64_t> bb, be;
-      DevBuf<int32_t> sorted;
-      if ((s = bb.reserve(hbig)) || (s = be.reserve(hbig)) || (s = sorted.reserve(nnz))) return bail(s);
-      k_big_bounds<<<grid_for(hbig), 256, 0, st>>>(hbig, big.p, r->roff.p, bb.p, be.p);
-      size_t tmp = 0;
-      cub::DeviceSegmentedSort::SortKeys(nullptr, tmp, r->radj.p, sorted.p, (int)nnz, hbig, bb.p, be.p, st);
-      DevBuf<char> t;
-      if ((s = t.reserve(tmp))) return bail(s);
-      cub::DeviceSegmentedSort::SortKeys(t.p, tmp, r->radj.p, sorted.p, (int)nnz, hbig, bb.p, be.p, st);
-      k_big_copy<<<std::min(hbig, num_sms() * 8), 256, 0, st>>>(hbig, bb.p, be.p, sorted.p, r->radj.p);
-    }
-  }
-  // does every stored edge point to a larger rank? (true for a degree-oriented DAG)
-  cudaMemsetAsync(down.p, 0, sizeof(int), st);
-  k_count_down<<<grid_for(n), 256, 0, st>>>(n, r->roff.p, r->radj.p, down.p);
-  int hdown = 0;
-  cudaMemcpyAsync(&hdown, down.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  k_incident<<<grid_for(n), 256, 0, st>>>(n, r->order.p, rdeg.p, indeg.p, inc.p);
+  if ((s = scan_i64(n, inc.p, r->rinc.p, st))) return bail(s);
+  cudaMemcpyAsync(&r->nin, r->rinc.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+  // gather + sort in one pass; lists longer than kSortCap get a segmented
+  // sort of their own afterwards
+  cudaMemsetAsync(nbig.p, 0, sizeof(int), st);
+  k_rank_gather_sort<<<grid_for(n * 32, kGatherWarps * 32), kGatherWarps * 32, 0, st>>>(
+      n, r->order.p, rank.p, g->off.p, g->adj.p, r->roff.p, r->radj.p, big.p, nbig.p);
+  int hbig = 0;
+  cudaMemcpyAsync(&hbig, nbig.p, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank relabel: ") + cudaGetErrorString(e)));
-  r->upward = hdown == 0;
+  if ((s = finish_rank_graph(r, n, nnz, big.p, hbig, st))) return bail(s);
   g->rg = r;
   return GPM_OK;
 }
@@ -639,7 +840,7 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
 
 int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, cudaStream_t st, RankPlan **out) {
   GPM_TRY(ensure_rank_graph(g, st));
-  const int64_t n = g->n, nnz = g->nnz;
+  const int64_t n = g->n;
   RankPlan *p = new RankPlan();
   p->cta_min = cta_min;
   p->long_min = long_min;
@@ -648,28 +849,21 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
     return s;
   };
   int s;
-  if ((s = p->poff.reserve(n + 1)) || (s = p->pseg.reserve(nnz)) || (s = p->plong.reserve(n)) ||
-      (s = p->counters.reserve(4)))
+  const int64_t nin = g->rg->nin;
+  if ((s = p->poff.reserve(n + 1)) || (s = p->pseg.reserve(std::max<int64_t>(nin, 1))) ||
+      (s = p->plong.reserve(n)) || (s = p->pshort.reserve(n)) || (s = p->counters.reserve(4)))
     return bail(s);
   const int64_t *roff = g->rg->roff.p;
   const int32_t *radj = g->rg->radj.p;
-  // 2. owner / segment CSR
-  DevBuf<int32_t> nshort, slen;
-  DevBuf<int64_t> tot, sstart;
-  DevBuf<unsigned long long> curl, curs, work;
-  if ((s = nshort.reserve(n)) || (s = tot.reserve(n)) || (s = curl.reserve(n)) || (s = curs.reserve(n)) ||
-      (s = work.reserve(n)) || (s = sstart.reserve(nnz)) || (s = slen.reserve(nnz)))
-    return bail(s);
+  // 2. segments placed in their owners' rooms, one pass
+  DevBuf<unsigned long long> work;
+  if ((s = work.reserve(n))) return bail(s);
+  cudaMemcpyAsync(p->poff.p, g->rg->rinc.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice, st);
   cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
-  cudaMemsetAsync(nshort.p, 0, sizeof(int32_t) * n, st);
+  cudaMemsetAsync(p->pshort.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
-  k_partner_count<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, g->rg->upward, long_min, cfg, p->plong.p,
-                                                     nshort.p, sstart.p, slen.p);
-  k_partner_sizes<<<grid_for(n), 256, 0, st>>>(n, p->plong.p, nshort.p, tot.p);
-  if ((s = scan_i64(n, tot.p, p->poff.p, st))) return bail(s);
-  k_partner_cursors<<<grid_for(n), 256, 0, st>>>(n, p->poff.p, p->plong.p, curl.p, curs.p);
-  k_partner_fill<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, long_min, cfg, sstart.p, slen.p, curl.p,
-                                                    curs.p, p->pseg.p, work.p);
+  k_partner_place<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, g->rg->upward, long_min, cfg, p->poff.p,
+                                                     p->plong.p, p->pshort.p, p->pseg.p, work.p);
   // 3. task queues, heaviest first
   DevBuf<unsigned long long> ckey, wkey;
   DevBuf<int32_t> cval, wval;
@@ -678,7 +872,8 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
       (s = sizes.reserve(2)) || (s = p->cta_tasks.reserve(n)) || (s = p->warp_tasks.reserve(n)))
     return bail(s);
   cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st);
-  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->poff.p, work.p, cta_min, cfg, ckey.p, cval.p, wkey.p,
+  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->plong.p, p->pshort.p, work.p, cta_min, cfg, ckey.p, cval.p,
+                                            wkey.p,
                                             wval.p, sizes.p);
   int h[2] = {0, 0};
   cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st);
@@ -712,10 +907,11 @@ int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long l
   GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 4 * sizeof(int), st));
   if (rec)
     k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p,
-                                                           p->plong.p, p->cta_tasks.p, p->n_cta, p->warp_tasks.p,
+                                                           p->plong.p, p->pshort.p, p->cta_tasks.p, p->n_cta, p->warp_tasks.p,
                                                            p->n_warp, p->counters.p, d_out, rec);
   else
     k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p, p->plong.p,
+                                                   p->pshort.p,
                                                    p->cta_tasks.p, p->n_cta, p->warp_tasks.p, p->n_warp,
                                                    p->counters.p, d_out, nullptr);
   GPM_LAUNCH_CHECK();
@@ -731,16 +927,24 @@ int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
 }
 
 // out[0] segments, out[1] keys in them, out[2] keys of the owners' lists
-__global__ void k_plan_stats(int64_t nseg, const longlong2 *__restrict__ pseg, const int32_t *__restrict__ tasks,
-                             int ntasks, const int64_t *__restrict__ roff, unsigned long long *__restrict__ out) {
-  unsigned long long keys = 0, okeys = 0;
-  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nseg; j += (int64_t)gridDim.x * blockDim.x)
-    keys += (unsigned long long)(pseg[j].y - pseg[j].x);
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntasks; t += (int64_t)gridDim.x * blockDim.x)
-    okeys += (unsigned long long)(roff[tasks[t] + 1] - roff[tasks[t]]);
+__global__ void k_plan_stats(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
+                             const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
+                             const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
+                             unsigned long long *__restrict__ out) {
+  unsigned long long segs = 0, keys = 0, okeys = 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntasks; t += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t x = tasks[t];
+    okeys += (unsigned long long)(roff[x + 1] - roff[x]);
+    segs += (unsigned long long)(plong[x] + pshort[x]);
+    for (int64_t j = poff[x]; j < poff[x] + plong[x]; ++j) keys += (unsigned long long)(pseg[j].y - pseg[j].x);
+    for (int64_t j = poff[x + 1] - pshort[x]; j < poff[x + 1]; ++j)
+      keys += (unsigned long long)(pseg[j].y - pseg[j].x);
+  }
+  segs = warp_sum(segs);
   keys = warp_sum(keys);
   okeys = warp_sum(okeys);
   if (lane_id() == 0) {
+    atomicAdd(&out[0], segs);
     atomicAdd(&out[1], keys);
     atomicAdd(&out[2], okeys);
   }
@@ -751,18 +955,18 @@ int rank_plan_stats(gpm_graph *g, uint64_t *out) {
   if (g->nnz == 0) return GPM_OK;
   GPM_TRY(rank_build_plan(g, kRankCtaMin, kRankLongMin, 0));
   RankPlan *p = g->rank;
-  int64_t nseg = 0;
-  GPM_CUDA(cudaMemcpy(&nseg, p->poff.p + g->n, sizeof(int64_t), cudaMemcpyDeviceToHost));
   DevBuf<unsigned long long> o;
   GPM_TRY(o.reserve(3));
   GPM_CUDA(cudaMemset(o.p, 0, 24));
   const int grid = num_sms() * 8;
-  k_plan_stats<<<grid, 256>>>(nseg, p->pseg.p, p->cta_tasks.p, p->n_cta, g->rg->roff.p, o.p);
-  k_plan_stats<<<grid, 256>>>(0, p->pseg.p, p->warp_tasks.p, p->n_warp, g->rg->roff.p, o.p);
+  k_plan_stats<<<grid, 256>>>(p->cta_tasks.p, p->n_cta, g->rg->roff.p, p->poff.p, p->pseg.p, p->plong.p,
+                              p->pshort.p, o.p);
+  k_plan_stats<<<grid, 256>>>(p->warp_tasks.p, p->n_warp, g->rg->roff.p, p->poff.p, p->pseg.p, p->plong.p,
+                              p->pshort.p, o.p);
   GPM_LAUNCH_CHECK();
   unsigned long long h[3];
   GPM_CUDA(cudaMemcpy(h, o.p, sizeof h, cudaMemcpyDeviceToHost));
-  out[0] = (uint64_t)nseg;
+  out[0] = h[0];
   out[1] = h[1];
   out[2] = h[2];
   out[3] = (uint64_t)(p->n_cta + p->n_warp);

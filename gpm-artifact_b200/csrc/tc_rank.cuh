@@ -33,22 +33,28 @@ struct RankGraph {
   DevBuf<int64_t> roff;   // n + 1
   DevBuf<int32_t> radj;   // nnz
   DevBuf<int32_t> order;  // rank -> original id
+  // rinc[r] .. rinc[r+1]: one slot per stored edge incident to rank r (out
+  // or in); the triangle plan's segment room, nin = rinc[n]
+  DevBuf<int64_t> rinc;
+  int64_t nin = 0;
   int upward = 0;
 };
 
 // Per-graph schedule of GPM_TC_BITMAP (device arrays):
-//   poff/pseg   partner segments: for owner x, pseg[poff[x] .. poff[x+1])
-//               are [start, end) ranges of radj, each the part of one
-//               partner's list that lies inside [min N(x), max N(x)] (no
-//               key outside that range can be in N(x)); empty ranges are
-//               left out; the first plong[x] are long segments
+//   poff/pseg   partner segments: owner x has the room pseg[poff[x] ..
+//               poff[x+1]) (poff = rinc, one slot per incident edge); its
+//               plong[x] long segments fill the room from the front, its
+//               pshort[x] short ones from the back.  A segment is the
+//               [start, end) range of radj holding the part of one partner's
+//               list inside [min N(x), max N(x)] (no key outside that range
+//               can be in N(x)); empty ranges are left out
 //   cta_tasks / warp_tasks  owners by size class, heaviest first
 struct RankPlan {
   int cta_min = 0, long_min = 0;
   int n_cta = 0, n_warp = 0;
   DevBuf<int64_t> poff;
   DevBuf<longlong2> pseg;
-  DevBuf<int32_t> plong;
+  DevBuf<int32_t> plong, pshort;
   DevBuf<int32_t> cta_tasks, warp_tasks;
   DevBuf<int> counters;
 };
@@ -57,6 +63,12 @@ struct RankPlan {
 // graph and relabel it in one pass (the DAG's own id order is lost).
 int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid = nullptr, int ngraphs = 1,
                       bool upward_only = false);
+// The upward rank graph of a symmetric graph (orientation folded into the
+// relabel).  g->off must be on the device; with h_off/h_adj (host arrays,
+// pinned for overlap) the adjacency is uploaded into g->adj in chunks on a
+// copy stream, each chunk relabelled as soon as it lands; with nullptr,
+// g->adj is already on the device.
+int build_upward_rank_graph(gpm_graph *g, cudaStream_t st, const int64_t *h_off, const int32_t *h_adj);
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st);
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out);
 // out[0..3]: segments, keys in them, owner-list keys, owner tasks of the fixed plan
