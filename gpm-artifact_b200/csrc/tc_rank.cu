@@ -422,7 +422,10 @@ __global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, con
       int64_t os = own_u ? s : vs, oe = own_u ? e : ve;
       int64_t ps = own_u ? vs : s, pe = own_u ? ve : e;
       if (oe - os < 2) continue;
-      const int64_t lo = upward && own_u ? ps : lower_bound_key(radj, ps, pe, radj[os]);
+      // upward: when v owns the edge, every id of N(u) up to v sits at or
+      // before slot k, and min N(v) > v, so the search starts past k
+      const int64_t lo = upward ? (own_u ? ps : lower_bound_key(radj, k + 1, pe, radj[os]))
+                                : lower_bound_key(radj, ps, pe, radj[os]);
       const int64_t len = upper_bound_key(radj, lo, pe, radj[oe - 1]) - lo;
       if (len == 0) continue;
       const bool lng = len >= owner_long_min(cfg, owner, long_min);
@@ -719,10 +722,10 @@ int build_upward_rank_graph(gpm_graph *g, cudaStream_t st, const int64_t *h_off,
       (s = big.reserve(n)) || (s = nbig.reserve(1)) ||
       (s = nhubq.reserve(1)) || (s = hubcnt.reserve(n)) || (s = hubq.reserve(maxq)))
     return bail(s);
-  // vertex ranges of the adjacency chunks (about nsym / 8 edges each)
+  // vertex ranges of the adjacency chunks (about nsym / 16 edges each)
   std::vector<int64_t> cut{0};
   if (h_adj && nsym > 0) {
-    const int chunks = 8;
+    const int chunks = 16;
     for (int c = 1; c < chunks; ++c) {
       const int64_t want = nsym * c / chunks;
       int64_t v = std::lower_bound(h_off, h_off + n + 1, want) - h_off;
