@@ -125,9 +125,28 @@ class Graph {
 template <typename VID, typename VLABEL>
 class Loader {
  public:
-  // Loader::Load (io.h:22-33): "mtx" only; "txt"/"bin" are not implemented
-  // in the reference either (io.h:142-143)
+  // Loader::Load (io.h:22-33): "mtx", and "bin" -- a directory in the layout
+  // of scripts/gbin_reader (graph.vertex.bin / graph.edge.bin /
+  // graph.meta.txt), which the reference declares but leaves unimplemented
+  // (io.h:143); its stored pairs are taken as the mtx pairs are (self-loops
+  // dropped, ids already start at 0).  "txt" is unimplemented in both.
   void Load(std::string const &path, std::string const &format) {
+    if (format == "bin") {
+      int64_t n = 0, nnz = 0;
+      gpm_check(gpm_read_gbin(path.c_str(), &n, &nnz, nullptr, nullptr, nullptr), "Loader::Load");
+      std::vector<int64_t> off(n + 1);
+      std::vector<int32_t> idx(nnz > 0 ? nnz : 1);
+      gpm_check(gpm_read_gbin(path.c_str(), &n, &nnz, off.data(), idx.data(), nullptr), "Loader::Load");
+      vsize_ = (size_t)n;
+      vmin_ = 0;
+      edges_.clear();
+      edges_.reserve(nnz);
+      for (int64_t v = 0; v < n; ++v)
+        for (int64_t k = off[v]; k < off[v + 1]; ++k)
+          if (idx[k] != v) edges_.push_back({(VID)v, (VID)idx[k]});
+      vlabels_.clear();
+      return;
+    }
     if (format != "mtx") {
       std::fprintf(stderr, "F unknown or unimplemented format %s\n", format.c_str());
       std::abort();

@@ -1,4 +1,7 @@
-// Mirrors test/test_engine.cu: e-centric triangle count, labels loaded (and unused).
+// Mirrors test/test_engine.cu: e-centric triangle count, labels loaded (and
+// unused).  A directory as <graph_path> is read as a binary CSR ("bin").
+#include <sys/stat.h>
+
 #include <iostream>
 
 #include "antirf/antirf.h"
@@ -11,7 +14,9 @@ int main(int argc, char *argv[]) {
   }
   Loader<int, int> loader;
   Graph<int, int> hg;
-  loader.Load(argv[1], "mtx");
+  struct stat st;
+  const bool dir = stat(argv[1], &st) == 0 && S_ISDIR(st.st_mode);
+  loader.Load(argv[1], dir ? "bin" : "mtx");
   loader.LoadVLabel(argv[2]);
   loader.Build(hg);
   Engine<int, int> engine(hg, 1, TC, e_centric);

@@ -46,6 +46,9 @@ _SIGS = {
     "gpm_read_mtx": ([c_char_p, POINTER(c_int64), POINTER(c_int64), _P, _P, c_int64, POINTER(c_int32)], c_int),
     "gpm_read_labels": ([c_char_p, c_int64, c_int32, _P], c_int),
     "gpm_read_tve": ([c_char_p, POINTER(c_int64), POINTER(c_int64), _P, _P, _P, c_int64], c_int),
+    "gpm_read_gbin": ([c_char_p, POINTER(c_int64), POINTER(c_int64), _P, _P, POINTER(c_int32)], c_int),
+    "gpm_write_gbin": ([c_char_p, c_int64, _P, _P], c_int),
+    "gpm_convert_mtx_gbin": ([c_char_p, c_char_p], c_int),
     "gpm_gen_rmat": ([c_int, c_int, c_double, c_double, c_double, c_uint64, _P, _P], c_int),
     "gpm_gen_er": ([c_int64, c_int64, c_uint64, _P, _P], c_int),
     "gpm_gen_chung_lu": ([c_int64, c_double, c_double, c_uint64, POINTER(c_int64), _P, _P], c_int),
@@ -136,6 +139,28 @@ def read_mtx(path: str):
     check(lib.gpm_read_mtx(path.encode(), ctypes.byref(n), ctypes.byref(m), _ptr(src), _ptr(dst), m.value,
                            ctypes.byref(vmin)))
     return n.value, src, dst, vmin.value
+
+
+def read_gbin(prefix: str):
+    """Binary CSR (graph.vertex.bin / graph.edge.bin / graph.meta.txt):
+    (offsets int64[n+1], indices int32[nnz], max_degree)."""
+    n, m, md = c_int64(), c_int64(), c_int32()
+    check(lib.gpm_read_gbin(prefix.encode(), ctypes.byref(n), ctypes.byref(m), None, None, ctypes.byref(md)))
+    off = np.empty(n.value + 1, np.int64)
+    idx = np.empty(max(m.value, 1), np.int32)
+    check(lib.gpm_read_gbin(prefix.encode(), ctypes.byref(n), ctypes.byref(m), _ptr(off), _ptr(idx),
+                            ctypes.byref(md)))
+    return off, idx[: m.value], md.value
+
+
+def write_gbin(prefix: str, offsets, indices):
+    off = np.ascontiguousarray(offsets, np.int64)
+    idx = np.ascontiguousarray(indices, np.int32)
+    check(lib.gpm_write_gbin(prefix.encode(), len(off) - 1, _ptr(off), _ptr(idx) if len(idx) else None))
+
+
+def convert_mtx_gbin(mtx_path: str, prefix: str):
+    check(lib.gpm_convert_mtx_gbin(mtx_path.encode(), prefix.encode()))
 
 
 def read_labels(path: str, n: int, vmin: int = 0):

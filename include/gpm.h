@@ -82,12 +82,33 @@ int gpm_abi_version(void);
 int gpm_device_count(int *count);
 
 /* ---- file formats (host only, no device needed) ------------------------- */
-/* Loader::_load_mtx, src/graph/io.h:84-139: skip '%' comment lines, read the
- * "n n m" header, drop self-loops, shift ids by the minimum id.  Two-call
- * pattern: with src == NULL only *n and *m are returned.  *vmin receives the
- * id shift (needed by gpm_read_labels). */
+/* Loader::_load_mtx, src/graph/io.h:84-139: skip lines until one starts with
+ * a digit, read the "n n m" header, then integers in pairs (the rest of the
+ * second one's line ignored; a last line without a newline is not read),
+ * drop self-loops, shift ids by the minimum id.  Parsed on all host threads
+ * (line-parallel, with the exact sequential reading for irregular files).
+ * Two-call pattern: with src == NULL only *n and *m are returned (the parse
+ * is kept for the second call of the same thread).  *vmin receives the id
+ * shift (needed by gpm_read_labels). */
 int gpm_read_mtx(const char *path, int64_t *n, int64_t *m, int32_t *src, int32_t *dst,
                  int64_t cap, int32_t *vmin);
+/* Binary CSR in the layout the reference's converter writes
+ * (scripts/gbin_reader/greader.h:229-268; Loader::Load(..., "bin") is
+ * declared there but not implemented, io.h:143): <prefix>/graph.vertex.bin
+ * (int64 offsets, n+1), <prefix>/graph.edge.bin (int32 ids, nnz),
+ * <prefix>/graph.meta.txt ("n", "nnz", "4", "max degree").  Two-call pattern:
+ * with offsets == indices == NULL only the sizes (and *max_degree, may be
+ * NULL) are returned.  The arrays are checked (sizes, monotone offsets, ids in
+ * range) and returned as stored. */
+int gpm_read_gbin(const char *prefix, int64_t *n, int64_t *nnz, int64_t *offsets, int32_t *indices,
+                  int32_t *max_degree);
+/* Writes a CSR in that layout (creates the directory when missing). */
+int gpm_write_gbin(const char *prefix, int64_t n, const int64_t *offsets, const int32_t *indices);
+/* The reference converter (greader.cpp / greader.h:129-268) with its rules:
+ * "n n nnz" header, then each line split at single spaces and kept when it
+ * has exactly two tokens; self-loops kept; ids shifted by the minimum id;
+ * lists in file order. */
+int gpm_convert_mtx_gbin(const char *mtx_path, const char *prefix);
 /* Loader::LoadVLabel, src/graph/io.h:35-73: "v label" lines (v shifted by
  * vmin) or the literal "random<N>" (labels rand() % N with the C library's
  * rand(), as the reference does). */

@@ -97,3 +97,17 @@ def test_match_driver_hprd(tmp_path):
             f.writelines(f"v {v} {ql[v]} {qo[v + 1] - qo[v]}\n" for v in range(m))
             f.writelines(f"e {a} {b}\n" for a, b in zip(qs, qi) if a < b)
         assert f"#Embeddings: {int(z['expected'][i])}" in run("test_match", "-d", dpath, "-q", qpath)
+
+
+def test_engine_driver_reads_binary_csr(rmat_mtx, tmp_path):
+    """Loader::Load(path, "bin"): the graph written as a binary CSR (the
+    gbin_reader layout) gives the same count as the .mtx of the same graph."""
+    import gpm
+    path, off, idx, used = rmat_mtx
+    lab = tmp_path / "lab"
+    lab.write_text("".join(f"{v + 1} 0\n" for v in range(len(off) - 1)))
+    pre = str(tmp_path / "bin")
+    gpm.write_gbin(pre, off, idx)
+    tri = orc.tc(*orc.orient(off, idx))
+    assert f"Result: {tri}" in run("test_engine", path, lab)
+    assert f"Result: {tri}" in run("test_engine", pre, lab)
