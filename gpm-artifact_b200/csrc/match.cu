@@ -73,14 +73,20 @@ __device__ __forceinline__ void seg_range(const int64_t *__restrict__ off, const
   }
 }
 
-// n = number of (root, second vertex) pairs
+// n = number of (root, second vertex) pairs.  TRACK: every embedding found
+// takes a slot of *found; those below `limit` are written to emb_out (when
+// given: q.n data-vertex ids per embedding, in query-vertex order), and the
+// whole grid stops once `limit` are found (sub_ceci's -num,
+// myceci.cpp:615-617).  Otherwise the count goes to *out.
+template <bool TRACK>
 __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restrict__ pairs, int64_t n,
                                                const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
                                                const int32_t *__restrict__ ladj, const int32_t *__restrict__ loff,
                                                int L, const int32_t *__restrict__ labels,
                                                int32_t *__restrict__ scratch, int64_t maxd,
                                                unsigned long long *__restrict__ cursor,
-                                               unsigned long long *__restrict__ out) {
+                                               unsigned long long *__restrict__ out, unsigned long long limit,
+                                               unsigned long long *found, int32_t *__restrict__ emb_out) {
   const unsigned lane = lane_id();
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int32_t *lists = scratch + warp * maxd * (kMaxQ - 1);
@@ -94,6 +100,7 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restri
     if (lane == 0) r = atomicAdd(cursor, 1ull);
     r = __shfl_sync(0xffffffffu, r, 0);
     if (r >= (unsigned long long)n) break;
+    if (TRACK && *(volatile unsigned long long *)found >= limit) break;
     const int2 pr = pairs[r];
     emb[0] = pr.x;
     emb[1] = pr.y;
@@ -127,6 +134,17 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restri
           }
           unsigned m = __ballot_sync(0xffffffffu, ok);
           if (!last && ok) Lst[cnt + __popc(m & ((1u << lane) - 1u))] = x;
+          if (TRACK && last && m) {
+            unsigned long long at = 0;
+            if (lane == 0) at = atomicAdd(found, (unsigned long long)__popc(m));
+            at = __shfl_sync(0xffffffffu, at, 0);
+            const unsigned long long slot = at + __popc(m & ((1u << lane) - 1u));
+            if (emb_out && ok && slot < limit) {
+              int32_t *row = emb_out + slot * (unsigned long long)q.n;
+              for (int j = 0; j < depth; ++j) row[q.order[j]] = emb[j];
+              row[q.order[depth]] = x;
+            }
+          }
           cnt += __popc(m);
         }
         __syncwarp();
@@ -134,6 +152,7 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restri
           c += lane == 0 ? (unsigned long long)cnt : 0ull;
           --depth;
           build = false;
+          if (TRACK && *(volatile unsigned long long *)found >= limit) break;
           continue;
         }
         sz[depth] = cnt;
@@ -149,8 +168,30 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restri
       build = true;
     }
   }
+  if (TRACK) return;
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(out, c);
+}
+
+// Embeddings of a one- or two-vertex query into emb_out (slots below
+// limit): roots with the query root's label, or the materialised pairs.
+__global__ void k_list_small(QueryPlan q, int64_t n, const int32_t *__restrict__ labels, const int64_t *__restrict__ off,
+                             const int2 *__restrict__ pairs, int64_t npairs, unsigned long long limit,
+                             unsigned long long *__restrict__ found, int32_t *__restrict__ emb_out) {
+  const int64_t tot = q.n == 1 ? n : npairs;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    if (q.n == 1) {
+      if (labels[i] != q.label[0]) continue;
+      const unsigned long long slot = atomicAdd(found, 1ull);
+      if (slot < limit) emb_out[slot] = (int32_t)i;
+    } else {
+      const unsigned long long slot = atomicAdd(found, 1ull);
+      if (slot < limit) {
+        emb_out[slot * 2 + q.order[0]] = pairs[i].x;
+        emb_out[slot * 2 + q.order[1]] = pairs[i].y;
+      }
+    }
+  }
 }
 
 // (root, second) pairs: a warp per root with the query root's label; the
@@ -361,10 +402,20 @@ int gpm_query_destroy(gpm_query *q) {
   return GPM_OK;
 }
 
-int gpm_match(gpm_graph *g, const gpm_query *q, uint64_t *out) {
+}  // extern "C"
+
+namespace gpm {
+
+// The embeddings of q in g: counted (limit = ~0, emb = nullptr), counted up
+// to `limit`, or listed (emb: host array of limit * q->n ids).  *out = the
+// count, min(total, limit).
+static int match_run(gpm_graph *g, const gpm_query *q, unsigned long long limit, int32_t *emb, uint64_t *out) {
   if (!g || !q || !out) return fail(GPM_EINVAL, "gpm_match: NULL argument");
   if (!g->labels.p) return fail(GPM_EINVAL, "the data graph carries no labels");
   if (g->oriented) return fail(GPM_EINVAL, "matching needs the symmetric (unoriented) data graph");
+  const bool track = limit != ~0ull || emb;
+  *out = 0;
+  if (limit == 0) return GPM_OK;
   // label frequencies pick the root
   int maxl = 0;
   for (int i = 0; i < q->n; ++i) maxl = std::max(maxl, q->labels[i] + 1);
@@ -380,9 +431,26 @@ int gpm_match(gpm_graph *g, const gpm_query *q, uint64_t *out) {
   }
   QueryPlan plan;
   GPM_TRY(plan_query(q, freq, &plan));
-  if (q->n == 1) {
-    *out = (uint64_t)(plan.label[0] >= 0 && plan.label[0] < maxl ? freq[plan.label[0]] : 0);
+  DevBuf<unsigned long long> found;
+  DevBuf<int32_t> demb;
+  GPM_TRY(found.reserve(1));
+  GPM_CUDA(cudaMemset(found.p, 0, 8));
+  auto finish = [&](unsigned long long total) -> int {
+    const unsigned long long got = std::min<unsigned long long>(total, limit);
+    if (emb && got) GPM_CUDA(cudaMemcpy(emb, demb.p, sizeof(int32_t) * got * q->n, cudaMemcpyDeviceToHost));
+    *out = got;
     return GPM_OK;
+  };
+  if (emb) GPM_TRY(demb.reserve(std::max<unsigned long long>(1, limit) * q->n));
+  const int sblocks = (int)std::min<int64_t>((g->n + 255) / 256 + 1, (int64_t)num_sms() * 8);
+  if (q->n == 1) {
+    const unsigned long long total =
+        (unsigned long long)(plan.label[0] >= 0 && plan.label[0] < maxl ? freq[plan.label[0]] : 0);
+    if (emb && total) {
+      k_list_small<<<sblocks, 256>>>(plan, g->n, g->labels.p, g->off.p, nullptr, 0, limit, found.p, demb.p);
+      GPM_LAUNCH_CHECK();
+    }
+    return finish(total);
   }
   GPM_TRY(ensure_label_csr(g));
   LabelCsr *lc = g->lcsr;
@@ -398,16 +466,18 @@ int gpm_match(gpm_graph *g, const gpm_query *q, uint64_t *out) {
   GPM_LAUNCH_CHECK();
   unsigned long long np = 0;
   GPM_CUDA(cudaMemcpy(&np, npairs.p, 8, cudaMemcpyDeviceToHost));
-  if (q->n == 2 || np == 0) {
-    *out = np;
-    return GPM_OK;
-  }
+  if (np == 0 || (q->n == 2 && !emb)) return finish(np);
   DevBuf<int2> pairs;
   GPM_TRY(pairs.reserve(np));
   GPM_CUDA(cudaMemset(npairs.p, 0, 8));
   k_match_pairs<<<blocks, 256>>>(plan, g->n, g->off.p, lc->ladj.p, lc->loff.p, lc->L, g->labels.p, 0, pairs.p,
                                  npairs.p);
   GPM_LAUNCH_CHECK();
+  if (q->n == 2) {
+    k_list_small<<<sblocks, 256>>>(plan, g->n, g->labels.p, g->off.p, pairs.p, (int64_t)np, limit, found.p, demb.p);
+    GPM_LAUNCH_CHECK();
+    return finish(np);
+  }
   int64_t warps = (int64_t)num_sms() * 4 * 8;
   const int64_t cap_words = (int64_t)2 << 30;
   while (warps > 32 && warps * maxd * (kMaxQ - 1) > cap_words) warps >>= 1;
@@ -417,13 +487,33 @@ int gpm_match(gpm_graph *g, const gpm_query *q, uint64_t *out) {
   GPM_TRY(cursor.reserve(1));
   GPM_CUDA(cudaMemset(cursor.p, 0, 8));
   GPM_CUDA(cudaMemset(d.p, 0, 8));
-  k_match<<<(int)(warps / 8), 256>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p, lc->loff.p, lc->L,
-                                     g->labels.p, scratch.p, maxd, cursor.p, d.p);
+  if (track)
+    k_match<true><<<(int)(warps / 8), 256>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p, lc->loff.p,
+                                             lc->L, g->labels.p, scratch.p, maxd, cursor.p, d.p, limit, found.p,
+                                             emb ? demb.p : nullptr);
+  else
+    k_match<false><<<(int)(warps / 8), 256>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p,
+                                              lc->loff.p, lc->L, g->labels.p, scratch.p, maxd, cursor.p, d.p, limit,
+                                              found.p, nullptr);
   GPM_LAUNCH_CHECK();
   unsigned long long h = 0;
-  GPM_CUDA(cudaMemcpy(&h, d.p, 8, cudaMemcpyDeviceToHost));
-  *out = h;
-  return GPM_OK;
+  GPM_CUDA(cudaMemcpy(&h, track ? found.p : d.p, 8, cudaMemcpyDeviceToHost));
+  return finish(h);
+}
+
+}  // namespace gpm
+
+extern "C" {
+
+int gpm_match(gpm_graph *g, const gpm_query *q, uint64_t *out) { return match_run(g, q, ~0ull, nullptr, out); }
+
+int gpm_match_limit(gpm_graph *g, const gpm_query *q, uint64_t limit, uint64_t *out) {
+  return match_run(g, q, limit, nullptr, out);
+}
+
+int gpm_match_list(gpm_graph *g, const gpm_query *q, uint64_t limit, int32_t *emb, uint64_t *written) {
+  if (!emb && limit > 0) return fail(GPM_EINVAL, "gpm_match_list: NULL output");
+  return match_run(g, q, limit, emb, written);
 }
 
 }  // extern "C"

@@ -98,6 +98,8 @@ _SIGS = {
     "gpm_query_create": ([c_int64, c_int64, _P, _P, _P, POINTER(c_void_p)], c_int),
     "gpm_query_destroy": ([_P], c_int),
     "gpm_match": ([_P, _P, POINTER(c_uint64)], c_int),
+    "gpm_match_limit": ([_P, _P, c_uint64, POINTER(c_uint64)], c_int),
+    "gpm_match_list": ([_P, _P, c_uint64, _P, POINTER(c_uint64)], c_int),
 }
 for _name, (_args, _res) in _SIGS.items():
     if hasattr(lib, _name):
@@ -308,10 +310,21 @@ class Graph:
         check(lib.gpm_pattern(self.h, name.encode(), family, _ptr(counters), ctypes.byref(res)))
         return res.value, counters
 
-    def match(self, q: "Query") -> int:
+    def match(self, q: "Query", limit=None) -> int:
+        """Embeddings of q (sub_ceci semantics); with limit, min(total, limit)."""
         out = c_uint64()
-        check(lib.gpm_match(self.h, q.h, ctypes.byref(out)))
+        if limit is None:
+            check(lib.gpm_match(self.h, q.h, ctypes.byref(out)))
+        else:
+            check(lib.gpm_match_limit(self.h, q.h, int(limit), ctypes.byref(out)))
         return out.value
+
+    def match_list(self, q: "Query", limit):
+        """Up to `limit` embeddings, one row of q.n data-vertex ids each."""
+        emb = np.empty((max(int(limit), 1), q.n), np.int32)
+        out = c_uint64()
+        check(lib.gpm_match_list(self.h, q.h, int(limit), _ptr(emb), ctypes.byref(out)))
+        return emb[: out.value]
 
 
 class Sched:
@@ -467,6 +480,7 @@ class Batch:
 
 class Query:
     def __init__(self, n, src, dst, labels):
+        self.n = int(n)
         src, dst, lab = _i32(src), _i32(dst), _i32(labels)
         h = c_void_p()
         check(lib.gpm_query_create(n, len(src), _ptr(src), _ptr(dst), _ptr(lab), ctypes.byref(h)))

@@ -310,6 +310,15 @@ int gpm_query_destroy(gpm_query *q);
  * counts the same embeddings).  The data graph must be symmetric and carry
  * labels. */
 int gpm_match(gpm_graph *data, const gpm_query *q, uint64_t *out);
+/* sub_ceci's -num N (myceci.cpp:1021-1027, 615-617): enumeration stops once
+ * `limit` embeddings are found; *out = min(total, limit). */
+int gpm_match_limit(gpm_graph *data, const gpm_query *q, uint64_t limit, uint64_t *out);
+/* Embedding listing (no reference counterpart: sub_ceci counts and never
+ * prints its embeddings): up to `limit` embeddings into emb (host, limit * n
+ * int32), each the n data-vertex ids of query vertices 0..n-1; *written =
+ * min(total, limit).  All embeddings when total <= limit, otherwise an
+ * arbitrary `limit` of them. */
+int gpm_match_list(gpm_graph *data, const gpm_query *q, uint64_t limit, int32_t *emb, uint64_t *written);
 
 #ifdef __cplusplus
 }
