@@ -70,6 +70,10 @@ void orc_motif_bruteforce(int64_t n, const int64_t *off, const int32_t *idx, uin
  * (sub_ceci/myceci.cpp:540-668): the number of injective, label-preserving
  * maps of the query vertices into the data graph that map every query edge to
  * a data edge (non-induced; automorphic images counted separately). */
+/* Sum over DAG triangles u -> v -> w of wt[w] (with wt = out-degree: the
+ * last term of the 4-clique algorithmic byte count). */
+uint64_t orc_tc_weighted(int64_t n, const int64_t *doff, const int32_t *didx, const int64_t *wt, int threads);
+
 /* The CSR as 1-indexed Matrix Market coordinate text (the reference
  * loader's input, src/graph/io.h:22-153); bytes written or -1. */
 int64_t orc_write_mtx(const char *path, int64_t n, const int64_t *off, const int32_t *idx);

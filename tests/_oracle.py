@@ -27,6 +27,7 @@ def lib():
         L.orc_build_csr.restype = c_int64
         L.orc_orient.restype = c_int64
         L.orc_write_mtx.restype = c_int64
+        L.orc_tc_weighted.restype = c_uint64
         _lib = L
     return _lib
 
@@ -117,3 +118,9 @@ def write_mtx(path, off, idx):
     if r < 0:
         raise OSError(f"writing {path} failed")
     return r
+
+
+def tc_weighted(doff, didx, wt, threads=0):
+    """Sum over DAG triangles u -> v -> w of wt[w]."""
+    wt = np.ascontiguousarray(wt, np.int64)
+    return lib().orc_tc_weighted(c_int64(len(doff) - 1), _p(doff), _p(didx), _p(wt), c_int(threads))

@@ -119,3 +119,23 @@ def test_orientation_rule():
             want = deg[v] > deg[u] or (deg[v] == deg[u] and v > u)
             assert (int(v) in kept) == want
     assert len(didx) * 2 == len(idx)
+
+
+def test_weighted_triangle_sum():
+    """orc_tc_weighted with unit weights is the triangle count; with
+    out-degree weights it is checked against a plain loop."""
+    rng = np.random.default_rng(8)
+    n = 300
+    e = rng.integers(0, n, size=(2500, 2)).astype(np.int32)
+    off, idx = orc.build_csr(n, e[:, 0], e[:, 1])
+    doff, didx = orc.orient(off, idx)
+    assert orc.tc_weighted(doff, didx, np.ones(n, np.int64)) == orc.tc(doff, didx)
+    dp = np.diff(doff)
+    want = 0
+    for u in range(n):
+        nu = set(didx[doff[u]:doff[u + 1]].tolist())
+        for v in didx[doff[u]:doff[u + 1]]:
+            for w in didx[doff[v]:doff[v + 1]]:
+                if w in nu:
+                    want += int(dp[w])
+    assert orc.tc_weighted(doff, didx, dp.astype(np.int64)) == want
