@@ -154,6 +154,36 @@ def run_match(scale, seed=3):
     return res
 
 
+def run_match_scales(scales, budget_s, seed=3):
+    """The labelled workload at growing R-MAT scales (same label law, queries
+    walked on each graph): a query stops growing once one run took more than
+    budget_s / 8 seconds (the next scale costs several times more)."""
+    res = {"workload": "match_rmat_ef16_zipf8_scales", "budget_s": budget_s, "queries": {k: [] for k in SHAPES}}
+    alive = set(SHAPES)
+    for scale in scales:
+        if not alive:
+            break
+        n, s, d = gpm.gen_rmat(scale, 16, seed=seed)
+        lab = gpm.gen_zipf_labels(n, 8, 1.2, seed=seed)
+        g = gpm.Graph.from_edges(n, s, d, labels=lab)
+        off, idx = g.csr()
+        rng = np.random.default_rng(seed)
+        for name, shape in SHAPES.items():
+            ql = walk_query(off, idx, lab, shape, rng)
+            if name not in alive:
+                continue
+            e = np.array(shape[1], np.int32)
+            q = gpm.Query(shape[0], e[:, 0], e[:, 1], ql)
+            c, t = timed(lambda: g.match(q))
+            res["queries"][name].append({"scale": scale, "m": g.info().nnz // 2, "labels": ql.tolist(),
+                                         "matches": c, "s": t, "matches_per_s": c / t})
+            print(json.dumps({"scale": scale, "query": name, "matches": c, "s": round(t, 4)}), flush=True)
+            if t > budget_s / 8:
+                alive.discard(name)
+        g.close()
+    return res
+
+
 def batch_members(count, nmax, seed=5):
     rng = np.random.default_rng(seed)
     n = np.exp(rng.uniform(np.log(1e3), np.log(nmax), count)).astype(np.int64)
@@ -192,6 +222,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default="er,clique,motif,match,batch")
     ap.add_argument("--quick", action="store_true", help="smaller sizes for a smoke run")
+    ap.add_argument("--match-scales", default="", help="e.g. 16,18,20,21: the labelled workload at growing scales")
+    ap.add_argument("--match-budget", type=float, default=240.0, help="seconds a query may take at its last scale x 8")
     a = ap.parse_args()
     todo = a.only.split(",")
     if "er" in todo:
@@ -201,7 +233,11 @@ def main():
     if "motif" in todo:
         print(json.dumps(run_motif(14 if a.quick else 18)), flush=True)
     if "match" in todo:
-        print(json.dumps(run_match(12 if a.quick else 16)), flush=True)
+        if a.match_scales:
+            print(json.dumps(run_match_scales([int(x) for x in a.match_scales.split(",")], a.match_budget)),
+                  flush=True)
+        else:
+            print(json.dumps(run_match(12 if a.quick else 16)), flush=True)
     if "batch" in todo:
         print(json.dumps(run_batch(32 if a.quick else 256, 3e4 if a.quick else 1e6)), flush=True)
 
