@@ -73,6 +73,25 @@ __device__ __forceinline__ void seg_range(const int64_t *__restrict__ off, const
   }
 }
 
+// Is x in a's neighbours with label l?  Binary search inside a's label
+// segment (the whole list when the lists are not partitioned).
+__device__ __forceinline__ bool has_edge_label(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                                               const int32_t *__restrict__ ladj, const int32_t *__restrict__ loff,
+                                               int L, int32_t a, int l, int32_t x) {
+  if (L == 0) return has_edge(off, adj, a, x);
+  int64_t s, e;
+  seg_range(off, loff, L, a, l, &s, &e);
+  const int32_t *seg = ladj + off[a];
+  int64_t lo = s, hi = e - 1;
+  while (lo <= hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    const int32_t y = __ldg(seg + mid);
+    if (y == x) return true;
+    if (y < x) lo = mid + 1; else hi = mid - 1;
+  }
+  return false;
+}
+
 // n = number of (root, second vertex) pairs.  TRACK: every embedding found
 // takes a slot of *found; those below `limit` are written to emb_out (when
 // given: q.n data-vertex ids per embedding, in query-vertex order), and the
@@ -108,12 +127,29 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restri
     bool build = true;
     while (depth >= 2) {
       if (build) {
-        // candidates of position `depth`: the parent image's neighbours with
-        // the position's label (one segment of the label-partitioned list)
-        const int32_t pv = emb[q.parent_pos[depth]];
-        const int32_t *seg = ladj + off[pv];
+        // candidates of position `depth`: the neighbours with the position's
+        // label of whichever mapped query-neighbour has the fewest (one
+        // segment of the label-partitioned list); the other mapped
+        // query-neighbours are checked inside their own segments
+        const int lab = q.label[depth];
+        uint32_t nb = q.back_pos[depth] | (1u << q.parent_pos[depth]);
+        int src = q.parent_pos[depth];
         int64_t s, e;
-        seg_range(off, loff, L, pv, q.label[depth], &s, &e);
+        seg_range(off, loff, L, emb[src], lab, &s, &e);
+        if (L > 0 && q.back_pos[depth]) {
+          for (uint32_t bm = q.back_pos[depth]; bm; bm &= bm - 1) {
+            const int j = __ffs(bm) - 1;
+            int64_t sj, ej;
+            seg_range(off, loff, L, emb[j], lab, &sj, &ej);
+            if (ej - sj < e - s) {
+              src = j;
+              s = sj;
+              e = ej;
+            }
+          }
+        }
+        nb &= ~(1u << src);
+        const int32_t *seg = ladj + off[emb[src]];
         const bool last = depth == q.n - 1;
         int32_t *Lst = lists + (int64_t)(depth - 2) * maxd;
         int cnt = 0;
@@ -123,13 +159,13 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restri
           int32_t x = 0;
           if (i < e) {
             x = __ldg(seg + i);
-            ok = labels[x] == q.label[depth] && off[x + 1] - off[x] >= q.mindeg[depth];
+            ok = labels[x] == lab && off[x + 1] - off[x] >= q.mindeg[depth];
             for (int j = 0; ok && j < depth; ++j) ok = emb[j] != x;
-            uint32_t bm = q.back_pos[depth];
+            uint32_t bm = nb;
             while (ok && bm) {
               int j = __ffs(bm) - 1;
               bm &= bm - 1;
-              ok = has_edge(off, adj, emb[j], x);
+              ok = has_edge_label(off, adj, ladj, loff, L, emb[j], lab, x);
             }
           }
           unsigned m = __ballot_sync(0xffffffffu, ok);
