@@ -32,7 +32,13 @@ namespace gpm {
 constexpr int kCqWarpMax = 64;      // warp tasks: |L| <= 64
 constexpr int kCqCtaMax = 2048;     // CTA tasks: |L| <= 2048 (W <= 64)
 constexpr int kCqMaxK = 8;
-constexpr size_t kCqSmem = 96 * 1024;  // dynamic shared memory per CTA
+#ifndef GPM_CQ_SMEM_KB
+// 48 KB: 4 CTAs per SM.  R-MAT 20, median of 3: 4-cliques 55 ms, 5-cliques
+// 1.15 s, against 89 ms / 1.71 s at 96 KB (2 CTAs per SM, a quarter of the
+// warp slots); tasks whose rows do not fit use their CTA's global slab
+#define GPM_CQ_SMEM_KB 48
+#endif
+constexpr size_t kCqSmem = GPM_CQ_SMEM_KB * 1024;  // dynamic shared memory per CTA
 
 static int grid_for(int64_t work, int block = 256) {
   int64_t g = (work + block - 1) / block;
