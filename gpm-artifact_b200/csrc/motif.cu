@@ -26,6 +26,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "motif.cuh"
@@ -208,10 +209,30 @@ __global__ void k_edge_sums(int64_t n, const int64_t *__restrict__ roff, const i
 // Task x = highest-rank vertex of the cycle: for a in N(x) with a < x and
 // y in N(a) with y < x, cnt[y]++; the task adds sum_y C(cnt[y], 2).
 constexpr int kC4WarpCap = 512;  // (key, count) slots per warp -> tasks with bound <= 256
+constexpr int kC4CtaSlots = 8 * kC4WarpCap;  // a hub task's shared table: the 8 warps' tables together
+constexpr int kC4Probe = 16;                 // probes before a key goes to the global counters
+
+// Slot of y in a hub task's shared table: found or newly claimed within
+// kC4Probe probes, else -1 (y lives in the global counters).  A key never
+// moves once placed and a slot never changes key, so every thread agrees on
+// where y lives.
+__device__ __forceinline__ int c4_slot(int2 *tab, int32_t y, bool claim) {
+  uint32_t h = ((uint32_t)y * 2654435769u) >> (32 - 12);
+  for (int p = 0; p < kC4Probe; ++p) {
+    int cur = tab[h].x;
+    if (cur == -1 && claim) cur = atomicCAS(&tab[h].x, -1, y), cur = cur == -1 ? y : cur;
+    if (cur == y) return (int)h;
+    if (cur == -1) return -1;  // lookup only: an empty slot ends the probe sequence
+    h = (h + 1) & (kC4CtaSlots - 1);
+  }
+  return -1;
+}
 
 __global__ void k_c4_tasks(int64_t n, const int64_t *__restrict__ roff, const int64_t *__restrict__ split,
-                           const int32_t *__restrict__ radj, int warp_bound, int32_t *__restrict__ cta_tasks,
-                           int32_t *__restrict__ warp_tasks, int *__restrict__ sizes) {
+                           const int32_t *__restrict__ radj, int warp_bound, long long big_min,
+                           int32_t *__restrict__ cta_tasks, int32_t *__restrict__ warp_tasks,
+                           int32_t *__restrict__ big_tasks, unsigned long long *__restrict__ big_b,
+                           int *__restrict__ sizes) {
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const unsigned lane = lane_id();
@@ -222,9 +243,18 @@ __global__ void k_c4_tasks(int64_t n, const int64_t *__restrict__ roff, const in
       b += (unsigned long long)(roff[a + 1] - roff[a]);
     }
     b = warp_sum(b);
-    if (lane == 0 && split[x] - roff[x] >= 2) {
-      if (b > (unsigned long long)warp_bound) cta_tasks[atomicAdd(&sizes[0], 1)] = (int32_t)x;
-      else warp_tasks[atomicAdd(&sizes[1], 1)] = (int32_t)x;
+    const int64_t dx = split[x] - roff[x];
+    if (lane == 0 && dx >= 2) {
+      if (b > (unsigned long long)big_min) {
+        const int i = atomicAdd(&sizes[2], 1);
+        big_tasks[i] = (int32_t)x;
+        big_b[i] = b;
+        atomicMax(&sizes[3], (int)dx);
+      } else if (b > (unsigned long long)warp_bound) {
+        cta_tasks[atomicAdd(&sizes[0], 1)] = (int32_t)x;
+      } else {
+        warp_tasks[atomicAdd(&sizes[1], 1)] = (int32_t)x;
+      }
     }
   }
 }
@@ -240,7 +270,11 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
   const unsigned lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;
   unsigned *cnt = dense + (int64_t)blockIdx.x * dense_len;
-  // hub tasks: per-CTA dense counters in global memory, two passes
+  // hub tasks: counters in a shared-memory hash table; keys that find no slot
+  // within kC4Probe probes count in this CTA's dense global counters, and
+  // only then does a second pass settle (and re-zero) those
+  __shared__ int s_ovf;
+  static_assert(kC4CtaSlots == 4096, "c4_slot hashes to 12 bits");
   while (true) {
     if (threadIdx.x == 0) s_task = atomicAdd(&counters[0], 1);
     __syncthreads();
@@ -251,23 +285,42 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
     const int g = graph_of(gid, x);
     const int64_t base = gbase ? gbase[g] : 0;
     const int64_t a0 = roff[x], a1 = split[x];
-    for (int pass = 0; pass < 2; ++pass) {
-      unsigned long long c = 0;
+    for (int i = threadIdx.x; i < kC4CtaSlots; i += blockDim.x) c4sm[i] = make_int2(-1, 0);
+    if (threadIdx.x == 0) s_ovf = 0;
+    __syncthreads();
+    bool ovf = false;
+    for (int64_t k = a0 + wid; k < a1; k += 8) {
+      int32_t a = radj[k];
+      for (int64_t j = roff[a] + lane; j < roff[a + 1]; j += 32) {
+        int32_t y = __ldg(radj + j);
+        if (y >= x) break;
+        const int h = c4_slot(c4sm, y, true);
+        if (h >= 0) {
+          atomicAdd(&c4sm[h].y, 1);
+        } else {
+          atomicAdd(&cnt[y - base], 1u);
+          ovf = true;
+        }
+      }
+    }
+    if (ovf) s_ovf = 1;
+    __syncthreads();
+    unsigned long long c = 0;
+    for (int i = threadIdx.x; i < kC4CtaSlots; i += blockDim.x)
+      if (c4sm[i].x >= 0) c += choose2((unsigned long long)c4sm[i].y);
+    if (s_ovf) {
       for (int64_t k = a0 + wid; k < a1; k += 8) {
         int32_t a = radj[k];
         for (int64_t j = roff[a] + lane; j < roff[a + 1]; j += 32) {
           int32_t y = __ldg(radj + j);
           if (y >= x) break;
-          if (pass == 0) atomicAdd(&cnt[y - base], 1u);
-          else c += choose2(atomicExch(&cnt[y - base], 0u));
+          if (c4_slot(c4sm, y, false) < 0) c += choose2(atomicExch(&cnt[y - base], 0u));
         }
       }
-      if (pass == 1) {
-        c = warp_sum(c);
-        if (lane == 0 && c) atomicAdd(&acc[8 * g + 6], c);
-      }
-      __syncthreads();
     }
+    c = warp_sum(c);
+    if (lane == 0 && c) atomicAdd(&acc[8 * g + 6], c);
+    __syncthreads();
   }
   // tail tasks: shared-memory (key, count) table per warp
   int2 *tab = c4sm + wid * kC4WarpCap;
@@ -305,6 +358,218 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
     __syncwarp();
     c = warp_sum(c);
     if (lane == 0 && c) atomicAdd(&acc[8 * graph_of(gid, x) + 6], c);
+  }
+}
+
+// ------------------------------------------------------------ giant 4-cycle tasks
+// A task whose 2-hop bound passes big_min has far more distinct y than any
+// shared-memory table holds (nearly every wedge ends at its own y).  Its key
+// range [base, x) is cut into chunks that fit dense counters in shared memory
+// -- 16-bit halves of 32-bit words while x has fewer than 65536 neighbours
+// below it, so no count can carry into the next key.  Each a in N(x), a < x,
+// keeps a cursor into its sorted list, so a chunk walks only its own segment
+// [cur, first y >= hi) and records where it stopped.  Every increment adds
+// the counter's old value to the sum (C(c+1,2) - C(c,2) = c), so a chunk needs
+// no scan.  A dense chunk is then cleared by a vector memset, a sparse one by
+// re-walking the recorded segments.
+// Neighbours are handed out one at a time through a shared counter to lane
+// groups of P = 1..32 lanes (P grows as x has fewer neighbours below it); each
+// lane reads four keys per 16-byte load.  Lists far longer than the task's
+// mean are walked by whole warps.
+constexpr int kC4BigThreads = 1024;
+constexpr int kC4BigSmem = 200 * 1024;
+constexpr int kC4BigWords = kC4BigSmem / 4;
+
+struct C4Chunk {
+  const int32_t *radj;
+  int64_t nnz;  // radj length: 16-byte loads only inside it
+  int sh;
+  int32_t lo, hi;
+};
+
+// One step of a group of P lanes over a segment at j (< e): lane gl takes the
+// four keys at (j rounded down to 4) + 4 gl.  Keys at or after j that are
+// below hi and before e form a prefix of the step (the list is sorted); they
+// are counted into cw.  Returns the stop position (first key >= hi, or e)
+// when the segment ends inside the step, else -1.
+__device__ __forceinline__ int64_t c4_step(const C4Chunk &q, unsigned *cw, int64_t j, int64_t e, unsigned gl,
+                                           unsigned gfirst, unsigned gmask, unsigned gbits,
+                                           unsigned long long &c, unsigned &nw) {
+  const int64_t jb = j & ~(int64_t)3;
+  const int64_t p0 = jb + 4 * (int64_t)gl;
+  int32_t v[4];
+  if (p0 + 4 <= q.nnz) {
+    const int4 t = __ldg(reinterpret_cast<const int4 *>(q.radj + p0));
+    v[0] = t.x, v[1] = t.y, v[2] = t.z, v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = p0 + k < q.nnz ? __ldg(q.radj + p0 + k) : INT32_MAX;
+  }
+  const unsigned hmask = q.sh ? 0xffffu : 0xffffffffu;
+  const int64_t dj = j - p0, de = e - p0;
+  const int skip = dj <= 0 ? 0 : dj >= 4 ? 4 : (int)dj;  // keys of this lane before j
+  const int lim = de <= 0 ? 0 : de >= 4 ? 4 : (int)de;   // keys of this lane before e
+  int n_ok = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const bool ok = k >= skip && k < lim && v[k] < q.hi;
+    if (ok) {
+      const unsigned key = (unsigned)(v[k] - q.lo);
+      const unsigned w = key >> q.sh, s = (key & (unsigned)q.sh) << 4;
+      const unsigned old = atomicAdd(&cw[w], 1u << s);
+      c += (old >> s) & hmask;
+      ++n_ok;
+    }
+  }
+  nw += n_ok;
+  const bool out = skip + n_ok < 4;  // this lane saw the end of the segment
+  const unsigned has = (__ballot_sync(gmask, out) >> gfirst) & gbits;
+  if (!has) return -1;
+  const int rel = __shfl_sync(gmask, 4 * (int)gl + skip + n_ok, (int)gfirst + __ffs(has) - 1);
+  return jb + rel;
+}
+
+__global__ void __launch_bounds__(kC4BigThreads, 1)
+    k_c4_big(const int64_t *__restrict__ roff, const int64_t *__restrict__ split, const int32_t *__restrict__ radj,
+             int64_t nnz, const int32_t *__restrict__ gid, const int64_t *__restrict__ gbase,
+             const int32_t *__restrict__ tasks, const unsigned long long *__restrict__ task_b, int n_tasks,
+             int *__restrict__ counters, int64_t *__restrict__ scratch, int64_t scratch_len,
+             unsigned long long *__restrict__ acc) {
+  extern __shared__ __align__(16) unsigned cw[];
+  __shared__ int s_task, s_nlong, s_next, s_lnext;
+  __shared__ unsigned s_nw[2];
+  __shared__ unsigned long long s_sum;
+  // per-CTA scratch: cursor pairs (two arrays, swapped per chunk), list ends
+  // (bitwise-not for long lists), long-list indices
+  int64_t *cur = scratch + (int64_t)blockIdx.x * 4 * scratch_len;
+  int64_t *nxt = cur + scratch_len;
+  int64_t *end = nxt + scratch_len;
+  int32_t *lng = reinterpret_cast<int32_t *>(end + scratch_len);
+  const unsigned lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < kC4BigWords; i += blockDim.x) cw[i] = 0u;
+  C4Chunk q;
+  q.radj = radj;
+  q.nnz = nnz;
+  while (true) {
+    if (threadIdx.x == 0) {
+      s_task = atomicAdd(&counters[2], 1);
+      s_nlong = 0;
+      s_sum = 0;
+      s_next = 0;
+      s_lnext = 0;
+      s_nw[0] = s_nw[1] = 0;
+    }
+    __syncthreads();
+    const int t = s_task;
+    if (t >= n_tasks) break;
+    const int32_t x = tasks[t];
+    const int g = graph_of(gid, x);
+    const int64_t base = gbase ? gbase[g] : 0;
+    const int64_t a0 = roff[x];
+    const int dx = (int)(split[x] - a0);
+    q.sh = dx < 65536 ? 1 : 0;
+    int P = 1;
+    while (P < 32 && (int64_t)P * 2 * dx <= (int64_t)blockDim.x * 2) P *= 2;
+    const long long mean = (long long)(task_b[t] / (unsigned long long)dx);
+    const long long long_min = max(64ll * P, 2 * mean);
+    for (int i = threadIdx.x; i < dx; i += blockDim.x) {
+      const int32_t a = radj[a0 + i];
+      const int64_t s = roff[a], e = roff[a + 1];
+      cur[i] = s;
+      const bool lg = P < 32 && e - s > long_min;
+      end[i] = lg ? ~e : e;
+      if (lg) lng[atomicAdd(&s_nlong, 1)] = i;
+    }
+    __syncthreads();
+    const int nlong = s_nlong;
+    const int64_t keys = (int64_t)kC4BigWords << q.sh;
+    const unsigned gl = lane & (P - 1);
+    const unsigned gfirst = lane & ~(unsigned)(P - 1);
+    const unsigned gmask = P == 32 ? 0xffffffffu : (((1u << P) - 1) << gfirst);
+    const unsigned gbits = P == 32 ? 0xffffffffu : ((1u << P) - 1);
+    unsigned long long c = 0;
+    int parity = 0;
+    for (int64_t lo = base; lo < x; lo += keys, parity ^= 1) {
+      q.lo = (int32_t)lo;
+      q.hi = (int32_t)(lo + keys < (int64_t)x ? lo + keys : (int64_t)x);
+      unsigned nw = 0;
+      // long lists first, one warp each, handed out through s_lnext
+      while (true) {
+        int li = 0;
+        if (lane == 0) li = atomicAdd(&s_lnext, 1);
+        li = __shfl_sync(0xffffffffu, li, 0);
+        if (li >= nlong) break;
+        const int i = lng[li];
+        const int64_t e = ~end[i];
+        int64_t j = cur[i];
+        while (j < e) {
+          const int64_t stop = c4_step(q, cw, j, e, lane, 0, 0xffffffffu, 0xffffffffu, c, nw);
+          if (stop >= 0) {
+            j = stop;
+            break;
+          }
+          j = (j & ~(int64_t)3) + 128;
+        }
+        if (lane == 0) nxt[i] = j < e ? j : e;
+      }
+      // short lists: flattened walk, one step or one refill per iteration
+      {
+        int i = -1;
+        int64_t j = 0, e = 0;
+        while (true) {
+          if (j >= e) {
+            if (i >= 0 && gl == 0) nxt[i] = j;
+            int ni = 0;
+            if (gl == 0) ni = atomicAdd(&s_next, 1);
+            i = __shfl_sync(gmask, ni, gfirst);
+            if (i >= dx) break;
+            e = end[i];
+            j = cur[i];
+            if (e < 0) {  // long list: walked above
+              i = -1;
+              j = e = 0;
+            }
+            continue;
+          }
+          const int64_t stop = c4_step(q, cw, j, e, gl, gfirst, gmask, gbits, c, nw);
+          if (stop >= 0) j = e = stop;
+          else j = (j & ~(int64_t)3) + 4 * P;
+        }
+      }
+      nw = warp_sum(nw);
+      if (lane == 0 && nw) atomicAdd(&s_nw[parity], nw);
+      __syncthreads();
+      // clear: memset when dense, else re-walk [cur, nxt)
+      const bool dense = (unsigned long long)s_nw[parity] * 4 > (unsigned long long)kC4BigWords;
+      if (threadIdx.x == 0) {
+        s_next = 0;
+        s_lnext = 0;
+        s_nw[parity ^ 1] = 0;
+      }
+      if (dense) {
+        uint4 *v = reinterpret_cast<uint4 *>(cw);
+        for (int k = threadIdx.x; k < kC4BigWords / 4; k += blockDim.x) v[k] = make_uint4(0u, 0u, 0u, 0u);
+      } else {
+        for (int i = threadIdx.x; i < dx; i += blockDim.x) {
+          const int64_t j1 = nxt[i];
+          for (int64_t j = cur[i]; j < j1; ++j) cw[(unsigned)(__ldg(radj + j) - q.lo) >> q.sh] = 0u;
+        }
+      }
+      __syncthreads();
+      int64_t *tmp = cur;
+      cur = nxt;
+      nxt = tmp;
+    }
+    c = warp_sum(c);
+    if (lane == 0 && c) atomicAdd(&s_sum, c);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_sum) atomicAdd(&acc[8 * g + 6], s_sum);
+    // cur and nxt swap once per chunk: restore the base layout for the next task
+    if (cur != scratch + (int64_t)blockIdx.x * 4 * scratch_len) {
+      int64_t *tmp = cur;
+      cur = nxt;
+      nxt = tmp;
+    }
   }
 }
 
@@ -413,27 +678,60 @@ int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
   GPM_TRY(p->te.reserve(std::max<int64_t>(in.nnz, 1)));
   // queues of the per-edge triangle pass and of the 4-cycle pass
   DevBuf<int> sizes;
-  GPM_TRY(sizes.reserve(4));
+  GPM_TRY(sizes.reserve(6));
   GPM_TRY(p->te_ct.reserve(n));
   GPM_TRY(p->te_wt.reserve(n));
   GPM_TRY(p->c4_ct.reserve(n));
   GPM_TRY(p->c4_wt.reserve(n));
+  DevBuf<int32_t> bt;
+  DevBuf<unsigned long long> bb;
+  GPM_TRY(bt.reserve(n));
+  GPM_TRY(bb.reserve(n));
   GPM_TRY(p->te_counters.reserve(2));
-  GPM_TRY(p->c4_counters.reserve(2));
-  GPM_CUDA(cudaMemsetAsync(sizes.p, 0, 4 * sizeof(int), st));
+  GPM_TRY(p->c4_counters.reserve(4));
+  GPM_CUDA(cudaMemsetAsync(sizes.p, 0, 6 * sizeof(int), st));
   if (n > 0) {
     k_te_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->split.p, std::min(in.te_cta_min, kTeWarpCap / 2), p->te_ct.p, p->te_wt.p, sizes.p);
-    k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, p->split.p, radj, std::min(in.c4_warp_bound, kC4WarpCap / 2), p->c4_ct.p, p->c4_wt.p, sizes.p + 2);
+    const int wb = std::min(in.c4_warp_bound, kC4WarpCap / 2);
+    long long big_min = in.c4_big_min;
+    if (const char *e = getenv("GPM_C4_BIG_MIN")) big_min = atoll(e);
+    k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, p->split.p, radj, wb, std::max<long long>(big_min, (long long)wb),
+                                                 p->c4_ct.p, p->c4_wt.p, bt.p, bb.p, sizes.p + 2);
   }
-  int h[4];
+  int h[6];
   GPM_CUDA(cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st));
   GPM_CUDA(cudaStreamSynchronize(st));
   p->te_nc = h[0];
   p->te_nw = h[1];
   p->c4_nc = h[2];
   p->c4_nw = h[3];
+  p->c4_nb = h[4];
   p->te_grid = te_grid();
-  p->c4_grid = 2 * num_sms();
+  // giant tasks, largest bound first
+  GPM_TRY(p->c4_bt.reserve(std::max(p->c4_nb, 1)));
+  GPM_TRY(p->c4_bb.reserve(std::max(p->c4_nb, 1)));
+  if (p->c4_nb > 0) {
+    size_t tmp = 0;
+    GPM_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, bb.p, p->c4_bb.p, bt.p, p->c4_bt.p, p->c4_nb, 0,
+                                                       64, st));
+    DevBuf<char> t;
+    GPM_TRY(t.reserve(tmp));
+    GPM_CUDA(cub::DeviceRadixSort::SortPairsDescending(t.p, tmp, bb.p, p->c4_bb.p, bt.p, p->c4_bt.p, p->c4_nb, 0,
+                                                       64, st));
+    GPM_CUDA(cudaFuncSetAttribute(k_c4_big, cudaFuncAttributeMaxDynamicSharedMemorySize, kC4BigSmem));
+    int per_sm = 0;
+    GPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_big, kC4BigThreads, kC4BigSmem));
+    p->c4_big_grid = std::max(1, per_sm) * num_sms();
+    p->c4_scratch = std::max(h[5], 1);
+    // per CTA: cursors, next cursors, list ends (int64 each), long-list indices (int32, padded)
+    GPM_TRY(p->c4_cur.reserve((size_t)p->c4_scratch * 4 * p->c4_big_grid));
+    if ((reinterpret_cast<uintptr_t>(in.radj) & 15) != 0)
+      return fail(GPM_EINVAL, "motif: adjacency not 16-byte aligned");
+    GPM_CUDA(cudaStreamSynchronize(st));
+  }
+  // 4 CTAs per SM, fewer when the per-CTA dense counters would pass 8 GB
+  p->c4_grid = (int)std::max<int64_t>(
+      num_sms(), std::min<int64_t>(4 * num_sms(), ((int64_t)8 << 30) / (4 * std::max<int64_t>(in.max_graph_n, 1))));
   // per-CTA dense 4-cycle counters over the largest member graph; kept zero
   // between runs (the second pass of k_c4 clears what the first set)
   p->dense_len = std::max<int64_t>(in.max_graph_n, 1);
@@ -445,6 +743,20 @@ int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
   return GPM_OK;
 }
 
+// The 4-cycle launches: giant tasks first (largest bound first), then hub and tail tasks.
+static int c4_launch(MotifPlan *p, cudaStream_t st) {
+  const MotifInput &in = p->in;
+  if (p->c4_nb > 0)
+    k_c4_big<<<p->c4_big_grid, kC4BigThreads, kC4BigSmem, st>>>(
+        in.roff, p->split.p, in.radj, in.nnz, in.gid, in.gbase, p->c4_bt.p, p->c4_bb.p, p->c4_nb, p->c4_counters.p,
+        p->c4_cur.p, p->c4_scratch, p->acc.p);
+  if (p->c4_nc + p->c4_nw > 0)
+    k_c4<<<p->c4_grid, 256, 0, st>>>(in.roff, p->split.p, in.radj, in.gid, in.gbase, p->c4_ct.p, p->c4_nc,
+                                     p->c4_wt.p, p->c4_nw, p->c4_counters.p, p->dense.p, p->dense_len, p->acc.p);
+  GPM_LAUNCH_CHECK();
+  return GPM_OK;
+}
+
 // Launches only (capturable): zero the sums, triangles per edge, per-edge
 // and per-vertex sums, 4-cycles, 4-cliques, inversion.
 int motif_plan_run(MotifPlan *p, cudaStream_t st) {
@@ -453,15 +765,13 @@ int motif_plan_run(MotifPlan *p, cudaStream_t st) {
   GPM_CUDA(cudaMemsetAsync(p->acc.p, 0, sizeof(unsigned long long) * 8 * in.ngraphs, st));
   GPM_CUDA(cudaMemsetAsync(p->te.p, 0, sizeof(unsigned) * std::max<int64_t>(in.nnz, 1), st));
   GPM_CUDA(cudaMemsetAsync(p->te_counters.p, 0, 2 * sizeof(int), st));
-  GPM_CUDA(cudaMemsetAsync(p->c4_counters.p, 0, 2 * sizeof(int), st));
+  GPM_CUDA(cudaMemsetAsync(p->c4_counters.p, 0, 4 * sizeof(int), st));
   if (p->te_nc + p->te_nw > 0)
     k_edge_tri<<<p->te_grid, 256, kTeSmem, st>>>(in.roff, p->split.p, in.radj, p->te_ct.p, p->te_nc, p->te_wt.p,
                                                  p->te_nw, p->te_counters.p, p->te.p);
   if (n > 0)
     k_edge_sums<<<grid_for(n * 32), 256, 0, st>>>(n, in.roff, p->split.p, in.radj, p->te.p, in.gid, p->acc.p);
-  if (p->c4_nc + p->c4_nw > 0)
-    k_c4<<<p->c4_grid, 256, 0, st>>>(in.roff, p->split.p, in.radj, in.gid, in.gbase, p->c4_ct.p, p->c4_nc,
-                                     p->c4_wt.p, p->c4_nw, p->c4_counters.p, p->dense.p, p->dense_len, p->acc.p);
+  GPM_TRY(c4_launch(p, st));
   GPM_LAUNCH_CHECK();
   GPM_TRY(clique_plan_run(&p->k4, st));
   k_motif_combine<<<std::max(1, (in.ngraphs + 255) / 256), 256, 0, st>>>(in.ngraphs, p->acc.p, p->out.p);
@@ -478,10 +788,8 @@ int motif_plan_run_stage(MotifPlan *p, int stage, cudaStream_t st) {
       k_edge_tri<<<p->te_grid, 256, kTeSmem, st>>>(in.roff, p->split.p, in.radj, p->te_ct.p, p->te_nc, p->te_wt.p,
                                                    p->te_nw, p->te_counters.p, p->te.p);
   } else if (stage == 1) {
-    GPM_CUDA(cudaMemsetAsync(p->c4_counters.p, 0, 2 * sizeof(int), st));
-    if (p->c4_nc + p->c4_nw > 0)
-      k_c4<<<p->c4_grid, 256, 0, st>>>(in.roff, p->split.p, in.radj, in.gid, in.gbase, p->c4_ct.p, p->c4_nc,
-                                       p->c4_wt.p, p->c4_nw, p->c4_counters.p, p->dense.p, p->dense_len, p->acc.p);
+    GPM_CUDA(cudaMemsetAsync(p->c4_counters.p, 0, 4 * sizeof(int), st));
+    GPM_TRY(c4_launch(p, st));
   } else {
     GPM_TRY(clique_plan_run(&p->k4, st));
   }

@@ -17,8 +17,10 @@ struct MotifInput {
   // task-split thresholds (autotuned for batches): triangle-pass owners with
   // more than te_cta_min upward neighbours (<= 128) and 4-cycle tasks whose
   // 2-hop bound exceeds c4_warp_bound (<= 256) run on a CTA; clique tasks
-  // with more than cq_warp_max out-neighbours (<= 64) run on a CTA
+  // with more than cq_warp_max out-neighbours (<= 64) run on a CTA; 4-cycle
+  // tasks whose bound exceeds c4_big_min count in key-range chunks
   int te_cta_min = 128, c4_warp_bound = 256, cq_warp_max = 64;
+  long long c4_big_min = 4096;
 };
 
 // k-cliques of an upward graph (every list holds only larger ids); the count
@@ -55,8 +57,11 @@ struct MotifPlan {
   DevBuf<int32_t> dadj;
   int dag_max = 0;
   DevBuf<unsigned> te;
-  DevBuf<int32_t> te_ct, te_wt, c4_ct, c4_wt;
-  int te_nc = 0, te_nw = 0, c4_nc = 0, c4_nw = 0, te_grid = 0, c4_grid = 0;
+  DevBuf<int32_t> te_ct, te_wt, c4_ct, c4_wt, c4_bt;
+  DevBuf<unsigned long long> c4_bb;  // giant 4-cycle tasks and their 2-hop bounds, largest first
+  int te_nc = 0, te_nw = 0, c4_nc = 0, c4_nw = 0, c4_nb = 0, te_grid = 0, c4_grid = 0, c4_big_grid = 0;
+  DevBuf<int64_t> c4_cur;  // per-CTA cursors and list ends of the giant tasks
+  int64_t c4_scratch = 0;
   DevBuf<int> te_counters, c4_counters;
   DevBuf<unsigned> dense;
   int64_t dense_len = 0;

@@ -124,3 +124,46 @@ def tc_weighted(doff, didx, wt, threads=0):
     """Sum over DAG triangles u -> v -> w of wt[w]."""
     wt = np.ascontiguousarray(wt, np.int64)
     return lib().orc_tc_weighted(c_int64(len(doff) - 1), _p(doff), _p(didx), _p(wt), c_int(threads))
+
+
+def c4_two_hubs(off, idx, h0, h1):
+    """Non-induced 4-cycles of a graph whose only high-degree vertices are two
+    non-adjacent hubs h0, h1, without enumerating the hubs' neighbour pairs:
+    cycles avoiding both hubs (sum over vertex pairs of C(common, 2) / 2 from
+    the sparse square of the rest), cycles through one hub h (its opposite
+    vertex y has C(|N(y) & N(h)|, 2) of them) and cycles through both (pairs
+    of their common neighbours).  Test infrastructure only."""
+    import scipy.sparse as sp
+    n = len(off) - 1
+    src = np.repeat(np.arange(n), np.diff(off))
+    assert not np.any((src == h0) & (idx == h1)), "hubs must not be adjacent"
+    rest = (src != h0) & (src != h1) & (idx != h0) & (idx != h1)
+    A = sp.csr_matrix((np.ones(int(rest.sum()), np.int64), (src[rest], idx[rest])), shape=(n, n))
+    P = sp.triu(A @ A, k=1).tocoo()
+    c = P.data.astype(np.int64)
+    total = int((c * (c - 1) // 2).sum()) // 2
+    sets = []
+    for h in (h0, h1):
+        nb = idx[off[h]:off[h + 1]]
+        ind = np.zeros(n, np.int64)
+        ind[nb] = 1
+        t = A @ ind
+        total += int((t * (t - 1) // 2).sum())
+        sets.append(nb)
+    k = len(np.intersect1d(sets[0], sets[1]))
+    return total + k * (k - 1) // 2
+
+
+def two_hub_graph(n, m_rand, d0, d1, mids, seed):
+    """Random sparse graph on [2, n) with `mids` medium hubs (list of degrees,
+    vertices 2, 3, ...) and two non-adjacent hubs 0 and 1 of degrees d0, d1."""
+    rng = np.random.default_rng(seed)
+    e = rng.integers(2, n, size=(m_rand, 2))
+    parts = [e]
+    for i, dm in enumerate(mids):
+        parts.append(np.stack([np.full(dm, 2 + i), rng.integers(2, n, size=dm)], 1))
+    for h, dh in ((0, d0), (1, d1)):
+        nb = rng.choice(np.arange(2, n), size=dh, replace=False)
+        parts.append(np.stack([np.full(dh, h), nb], 1))
+    e = np.concatenate(parts).astype(np.int32)
+    return build_csr(n, e[:, 0], e[:, 1])

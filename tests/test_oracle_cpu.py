@@ -139,3 +139,14 @@ def test_weighted_triangle_sum():
                 if w in nu:
                     want += int(dp[w])
     assert orc.tc_weighted(doff, didx, dp.astype(np.int64)) == want
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_c4_two_hubs_formula_matches_oracle(seed):
+    """The closed-form 4-cycle count used for hub graphs too large for the
+    enumerating oracle agrees with it on small two-hub graphs."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(500, 3000))
+    off, idx = orc.two_hub_graph(n, 2 * n, n // 6, n // 15, [40, 70], seed=seed)
+    m4 = orc.motif4(off, idx)
+    assert orc.c4_two_hubs(off, idx, 0, 1) == int(m4[3] + m4[4] + 3 * m4[5])
