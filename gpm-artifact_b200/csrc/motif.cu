@@ -23,6 +23,7 @@
 // each sorted list is the degree-oriented DAG.  Every kernel takes an
 // optional per-vertex graph id so one launch serves a disjoint union of many
 // graphs (batch.cu) with per-graph accumulators.
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -33,6 +34,8 @@
 #include "tc_rank.cuh"
 
 namespace gpm {
+
+namespace cg = cooperative_groups;
 
 static int grid_for(int64_t work, int block = 256) {
   int64_t g = (work + block - 1) / block;
@@ -387,11 +390,33 @@ struct C4Chunk {
   int32_t lo, hi;
 };
 
+// Hash mode: a task whose bound is at most kC4HashMax counts in one pass in an
+// open-addressing table over the same shared memory, slots of (key + 1,
+// count) with 0 = empty, so a cleared array is an empty table and the dense
+// chunks find it zeroed.  The bound caps the distinct keys below the slot
+// count, so every probe sequence ends.
+constexpr unsigned kC4HashSlots = kC4BigWords / 2;
+constexpr unsigned long long kC4HashMax = kC4HashSlots * 6 / 10;
+__device__ __forceinline__ unsigned c4_hash_add(unsigned *cw, unsigned key1) {
+  unsigned h = (unsigned)(((unsigned long long)(key1 * 2654435761u) * kC4HashSlots) >> 32);
+  for (unsigned p = 0; p < kC4HashSlots; ++p) {
+    unsigned cur = cw[2 * h];
+    if (cur == 0u) {
+      cur = atomicCAS(&cw[2 * h], 0u, key1);
+      if (cur == 0u) cur = key1;
+    }
+    if (cur == key1) return atomicAdd(&cw[2 * h + 1], 1u);
+    if (++h == kC4HashSlots) h = 0;
+  }
+  return 0u;
+}
+
 // One step of a group of P lanes over a segment at j (< e): lane gl takes the
 // four keys at (j rounded down to 4) + 4 gl.  Keys at or after j that are
 // below hi and before e form a prefix of the step (the list is sorted); they
 // are counted into cw.  Returns the stop position (first key >= hi, or e)
 // when the segment ends inside the step, else -1.
+template <bool HASH>
 __device__ __forceinline__ int64_t c4_step(const C4Chunk &q, unsigned *cw, int64_t j, int64_t e, unsigned gl,
                                            unsigned gfirst, unsigned gmask, unsigned gbits,
                                            unsigned long long &c, unsigned &nw) {
@@ -415,9 +440,13 @@ __device__ __forceinline__ int64_t c4_step(const C4Chunk &q, unsigned *cw, int64
     const bool ok = k >= skip && k < lim && v[k] < q.hi;
     if (ok) {
       const unsigned key = (unsigned)(v[k] - q.lo);
-      const unsigned w = key >> q.sh, s = (key & (unsigned)q.sh) << 4;
-      const unsigned old = atomicAdd(&cw[w], 1u << s);
-      c += (old >> s) & hmask;
+      if (HASH) {
+        c += c4_hash_add(cw, key + 1);
+      } else {
+        const unsigned w = key >> q.sh, s = (key & (unsigned)q.sh) << 4;
+        const unsigned old = atomicAdd(&cw[w], 1u << s);
+        c += (old >> s) & hmask;
+      }
       ++n_ok;
     }
   }
@@ -482,7 +511,8 @@ __global__ void __launch_bounds__(kC4BigThreads, 1)
     }
     __syncthreads();
     const int nlong = s_nlong;
-    const int64_t keys = (int64_t)kC4BigWords << q.sh;
+    const bool hash = task_b[t] <= kC4HashMax;  // one pass over [base, x) in the hash table
+    const int64_t keys = hash ? (int64_t)x - base : (int64_t)kC4BigWords << q.sh;
     const unsigned gl = lane & (P - 1);
     const unsigned gfirst = lane & ~(unsigned)(P - 1);
     const unsigned gmask = P == 32 ? 0xffffffffu : (((1u << P) - 1) << gfirst);
@@ -503,7 +533,8 @@ __global__ void __launch_bounds__(kC4BigThreads, 1)
         const int64_t e = ~end[i];
         int64_t j = cur[i];
         while (j < e) {
-          const int64_t stop = c4_step(q, cw, j, e, lane, 0, 0xffffffffu, 0xffffffffu, c, nw);
+          const int64_t stop = hash ? c4_step<true>(q, cw, j, e, lane, 0, 0xffffffffu, 0xffffffffu, c, nw)
+                                    : c4_step<false>(q, cw, j, e, lane, 0, 0xffffffffu, 0xffffffffu, c, nw);
           if (stop >= 0) {
             j = stop;
             break;
@@ -520,9 +551,15 @@ __global__ void __launch_bounds__(kC4BigThreads, 1)
           if (j >= e) {
             if (i >= 0 && gl == 0) nxt[i] = j;
             int ni = 0;
-            if (gl == 0) ni = atomicAdd(&s_next, 1);
-            i = __shfl_sync(gmask, ni, gfirst);
-            if (i >= dx) break;
+            if (gl == 0) {  // one shared atomic for all group leaders of the warp that need an a
+              const cg::coalesced_group ct = cg::coalesced_threads();
+              int base = 0;
+              if (ct.thread_rank() == 0) base = atomicAdd(&s_next, (int)ct.size());
+              ni = ct.shfl(base, 0) + (int)ct.thread_rank();
+            }
+            ni = __shfl_sync(gmask, ni, gfirst);
+            if (ni >= dx) break;
+            i = dx - 1 - ni;  // highest rank (longest lists) first
             e = end[i];
             j = cur[i];
             if (e < 0) {  // long list: walked above
@@ -531,7 +568,8 @@ __global__ void __launch_bounds__(kC4BigThreads, 1)
             }
             continue;
           }
-          const int64_t stop = c4_step(q, cw, j, e, gl, gfirst, gmask, gbits, c, nw);
+          const int64_t stop = hash ? c4_step<true>(q, cw, j, e, gl, gfirst, gmask, gbits, c, nw)
+                                    : c4_step<false>(q, cw, j, e, gl, gfirst, gmask, gbits, c, nw);
           if (stop >= 0) j = e = stop;
           else j = (j & ~(int64_t)3) + 4 * P;
         }
@@ -540,7 +578,7 @@ __global__ void __launch_bounds__(kC4BigThreads, 1)
       if (lane == 0 && nw) atomicAdd(&s_nw[parity], nw);
       __syncthreads();
       // clear: memset when dense, else re-walk [cur, nxt)
-      const bool dense = (unsigned long long)s_nw[parity] * 4 > (unsigned long long)kC4BigWords;
+      const bool dense = hash || (unsigned long long)s_nw[parity] * 4 > (unsigned long long)kC4BigWords;
       if (threadIdx.x == 0) {
         s_next = 0;
         s_lnext = 0;
@@ -674,7 +712,7 @@ int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
   GPM_TRY(p->out.reserve(8 * (size_t)in.ngraphs));
   GPM_TRY(p->split.reserve(n));
   if (n > 0) k_split<<<grid_for(n), 256, 0, st>>>(n, roff, radj, p->split.p);
-  GPM_TRY(dag_from_split(n, roff, p->split.p, radj, p->doff, p->dadj, &p->dag_max, st));
+  if (in.size == 4) GPM_TRY(dag_from_split(n, roff, p->split.p, radj, p->doff, p->dadj, &p->dag_max, st));
   GPM_TRY(p->te.reserve(std::max<int64_t>(in.nnz, 1)));
   // queues of the per-edge triangle pass and of the 4-cycle pass
   DevBuf<int> sizes;
@@ -692,11 +730,13 @@ int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
   GPM_CUDA(cudaMemsetAsync(sizes.p, 0, 6 * sizeof(int), st));
   if (n > 0) {
     k_te_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->split.p, std::min(in.te_cta_min, kTeWarpCap / 2), p->te_ct.p, p->te_wt.p, sizes.p);
-    const int wb = std::min(in.c4_warp_bound, kC4WarpCap / 2);
-    long long big_min = in.c4_big_min;
-    if (const char *e = getenv("GPM_C4_BIG_MIN")) big_min = atoll(e);
-    k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, p->split.p, radj, wb, std::max<long long>(big_min, (long long)wb),
-                                                 p->c4_ct.p, p->c4_wt.p, bt.p, bb.p, sizes.p + 2);
+    if (in.size == 4) {
+      const int wb = std::min(in.c4_warp_bound, kC4WarpCap / 2);
+      long long big_min = in.c4_big_min;
+      if (const char *e = getenv("GPM_C4_BIG_MIN")) big_min = atoll(e);
+      k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, p->split.p, radj, wb, std::max<long long>(big_min, (long long)wb),
+                                                   p->c4_ct.p, p->c4_wt.p, bt.p, bb.p, sizes.p + 2);
+    }
   }
   int h[6];
   GPM_CUDA(cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st));
@@ -707,6 +747,10 @@ int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
   p->c4_nw = h[3];
   p->c4_nb = h[4];
   p->te_grid = te_grid();
+  if (in.size == 3) {
+    GPM_CUDA(cudaStreamSynchronize(st));
+    return GPM_OK;
+  }
   // giant tasks, largest bound first
   GPM_TRY(p->c4_bt.reserve(std::max(p->c4_nb, 1)));
   GPM_TRY(p->c4_bb.reserve(std::max(p->c4_nb, 1)));
@@ -771,9 +815,10 @@ int motif_plan_run(MotifPlan *p, cudaStream_t st) {
                                                  p->te_nw, p->te_counters.p, p->te.p);
   if (n > 0)
     k_edge_sums<<<grid_for(n * 32), 256, 0, st>>>(n, in.roff, p->split.p, in.radj, p->te.p, in.gid, p->acc.p);
-  GPM_TRY(c4_launch(p, st));
-  GPM_LAUNCH_CHECK();
-  GPM_TRY(clique_plan_run(&p->k4, st));
+  if (in.size == 4) {
+    GPM_TRY(c4_launch(p, st));
+    GPM_TRY(clique_plan_run(&p->k4, st));
+  }
   k_motif_combine<<<std::max(1, (in.ngraphs + 255) / 256), 256, 0, st>>>(in.ngraphs, p->acc.p, p->out.p);
   GPM_LAUNCH_CHECK();
   return GPM_OK;
@@ -812,6 +857,7 @@ extern "C" int gpm_motif(gpm_graph *g, int k, uint64_t *out) {
   in.roff = g->rg->roff.p;
   in.radj = g->rg->radj.p;
   in.max_graph_n = g->n;
+  in.size = k;
   MotifPlan plan;
   GPM_TRY(motif_plan_build(in, &plan, 0));
   GPM_TRY(motif_plan_run(&plan, 0));

@@ -21,6 +21,7 @@ struct MotifInput {
   // tasks whose bound exceeds c4_big_min count in key-range chunks
   int te_cta_min = 128, c4_warp_bound = 256, cq_warp_max = 64;
   long long c4_big_min = 4096;
+  int size = 4;  // 3: only the per-edge triangle pass and the degree sums (out[0..1])
 };
 
 // k-cliques of an upward graph (every list holds only larger ids); the count
