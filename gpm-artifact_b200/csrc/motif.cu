@@ -213,19 +213,21 @@ __global__ void k_edge_sums(int64_t n, const int64_t *__restrict__ roff, const i
 // y in N(a) with y < x, cnt[y]++; the task adds sum_y C(cnt[y], 2).
 constexpr int kC4WarpCap = 512;  // (key, count) slots per warp -> tasks with bound <= 256
 constexpr int kC4CtaSlots = 8 * kC4WarpCap;  // a hub task's shared table: the 8 warps' tables together
-constexpr int kC4Probe = 16;                 // probes before a key goes to the global counters
+// Hub tasks have a 2-hop bound of at most kC4HubMax (larger ones go to
+// k_c4_big), so at most that many distinct keys meet kC4CtaSlots slots: the
+// table never fills and every probe sequence ends.
+constexpr long long kC4HubMax = kC4CtaSlots * 3 / 4;
 
-// Slot of y in a hub task's shared table: found or newly claimed within
-// kC4Probe probes, else -1 (y lives in the global counters).  A key never
-// moves once placed and a slot never changes key, so every thread agrees on
-// where y lives.
-__device__ __forceinline__ int c4_slot(int2 *tab, int32_t y, bool claim) {
+// Slot of y in a hub task's shared table, found or newly claimed.
+__device__ __forceinline__ int c4_slot(int2 *tab, int32_t y) {
   uint32_t h = ((uint32_t)y * 2654435769u) >> (32 - 12);
-  for (int p = 0; p < kC4Probe; ++p) {
+  for (int p = 0; p < kC4CtaSlots; ++p) {
     int cur = tab[h].x;
-    if (cur == -1 && claim) cur = atomicCAS(&tab[h].x, -1, y), cur = cur == -1 ? y : cur;
+    if (cur == -1) {
+      cur = atomicCAS(&tab[h].x, -1, y);
+      if (cur == -1) cur = y;
+    }
     if (cur == y) return (int)h;
-    if (cur == -1) return -1;  // lookup only: an empty slot ends the probe sequence
     h = (h + 1) & (kC4CtaSlots - 1);
   }
   return -1;
@@ -266,17 +268,12 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
                                             const int32_t *__restrict__ radj, const int32_t *__restrict__ gid,
                                             const int64_t *__restrict__ gbase, const int32_t *__restrict__ cta_tasks,
                                             int n_cta, const int32_t *__restrict__ warp_tasks, int n_warp,
-                                            int *__restrict__ counters, unsigned *__restrict__ dense,
-                                            int64_t dense_len, unsigned long long *__restrict__ acc) {
+                                            int *__restrict__ counters, unsigned long long *__restrict__ acc) {
   __shared__ int2 c4sm[8 * kC4WarpCap];
   __shared__ int s_task;
   const unsigned lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;
-  unsigned *cnt = dense + (int64_t)blockIdx.x * dense_len;
-  // hub tasks: counters in a shared-memory hash table; keys that find no slot
-  // within kC4Probe probes count in this CTA's dense global counters, and
-  // only then does a second pass settle (and re-zero) those
-  __shared__ int s_ovf;
+  // hub tasks: counters in a shared-memory hash table over the 8 warps' tables
   static_assert(kC4CtaSlots == 4096, "c4_slot hashes to 12 bits");
   while (true) {
     if (threadIdx.x == 0) s_task = atomicAdd(&counters[0], 1);
@@ -286,41 +283,22 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
     if (t >= n_cta) break;
     const int32_t x = cta_tasks[t];
     const int g = graph_of(gid, x);
-    const int64_t base = gbase ? gbase[g] : 0;
     const int64_t a0 = roff[x], a1 = split[x];
     for (int i = threadIdx.x; i < kC4CtaSlots; i += blockDim.x) c4sm[i] = make_int2(-1, 0);
-    if (threadIdx.x == 0) s_ovf = 0;
     __syncthreads();
-    bool ovf = false;
     for (int64_t k = a0 + wid; k < a1; k += 8) {
       int32_t a = radj[k];
       for (int64_t j = roff[a] + lane; j < roff[a + 1]; j += 32) {
         int32_t y = __ldg(radj + j);
         if (y >= x) break;
-        const int h = c4_slot(c4sm, y, true);
-        if (h >= 0) {
-          atomicAdd(&c4sm[h].y, 1);
-        } else {
-          atomicAdd(&cnt[y - base], 1u);
-          ovf = true;
-        }
+        const int h = c4_slot(c4sm, y);
+        if (h >= 0) atomicAdd(&c4sm[h].y, 1);
       }
     }
-    if (ovf) s_ovf = 1;
     __syncthreads();
     unsigned long long c = 0;
     for (int i = threadIdx.x; i < kC4CtaSlots; i += blockDim.x)
       if (c4sm[i].x >= 0) c += choose2((unsigned long long)c4sm[i].y);
-    if (s_ovf) {
-      for (int64_t k = a0 + wid; k < a1; k += 8) {
-        int32_t a = radj[k];
-        for (int64_t j = roff[a] + lane; j < roff[a + 1]; j += 32) {
-          int32_t y = __ldg(radj + j);
-          if (y >= x) break;
-          if (c4_slot(c4sm, y, false) < 0) c += choose2(atomicExch(&cnt[y - base], 0u));
-        }
-      }
-    }
     c = warp_sum(c);
     if (lane == 0 && c) atomicAdd(&acc[8 * g + 6], c);
     __syncthreads();
@@ -734,7 +712,8 @@ int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
       const int wb = std::min(in.c4_warp_bound, kC4WarpCap / 2);
       long long big_min = in.c4_big_min;
       if (const char *e = getenv("GPM_C4_BIG_MIN")) big_min = atoll(e);
-      k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, p->split.p, radj, wb, std::max<long long>(big_min, (long long)wb),
+      big_min = std::min(std::max<long long>(big_min, (long long)wb), kC4HubMax);
+      k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, p->split.p, radj, wb, big_min,
                                                    p->c4_ct.p, p->c4_wt.p, bt.p, bb.p, sizes.p + 2);
     }
   }
@@ -773,14 +752,11 @@ int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
       return fail(GPM_EINVAL, "motif: adjacency not 16-byte aligned");
     GPM_CUDA(cudaStreamSynchronize(st));
   }
-  // 4 CTAs per SM, fewer when the per-CTA dense counters would pass 8 GB
-  p->c4_grid = (int)std::max<int64_t>(
-      num_sms(), std::min<int64_t>(4 * num_sms(), ((int64_t)8 << 30) / (4 * std::max<int64_t>(in.max_graph_n, 1))));
-  // per-CTA dense 4-cycle counters over the largest member graph; kept zero
-  // between runs (the second pass of k_c4 clears what the first set)
-  p->dense_len = std::max<int64_t>(in.max_graph_n, 1);
-  GPM_TRY(p->dense.reserve((size_t)p->dense_len * p->c4_grid));
-  GPM_CUDA(cudaMemsetAsync(p->dense.p, 0, sizeof(unsigned) * (size_t)p->dense_len * p->c4_grid, st));
+  {
+    int per_sm = 0;
+    GPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4, 256, 0));
+    p->c4_grid = std::max(1, per_sm) * num_sms();
+  }
   GPM_TRY(clique_plan_build(&p->k4, n, p->doff.p, p->dadj.p, p->dag_max, 4, in.gid, p->acc.p, 8, 5, st,
                             in.cq_warp_max));
   GPM_CUDA(cudaStreamSynchronize(st));
@@ -796,7 +772,7 @@ static int c4_launch(MotifPlan *p, cudaStream_t st) {
         p->c4_cur.p, p->c4_scratch, p->acc.p);
   if (p->c4_nc + p->c4_nw > 0)
     k_c4<<<p->c4_grid, 256, 0, st>>>(in.roff, p->split.p, in.radj, in.gid, in.gbase, p->c4_ct.p, p->c4_nc,
-                                     p->c4_wt.p, p->c4_nw, p->c4_counters.p, p->dense.p, p->dense_len, p->acc.p);
+                                     p->c4_wt.p, p->c4_nw, p->c4_counters.p, p->acc.p);
   GPM_LAUNCH_CHECK();
   return GPM_OK;
 }

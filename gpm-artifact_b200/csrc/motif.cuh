@@ -13,14 +13,15 @@ struct MotifInput {
   const int32_t *gid = nullptr;    // per-vertex graph index (nullptr: one graph)
   const int64_t *gbase = nullptr;  // per-graph first vertex (nullptr: 0)
   int ngraphs = 1;
-  int64_t max_graph_n = 0;         // largest member graph (sizes 4-cycle counters)
+  int64_t max_graph_n = 0;         // largest member graph
   // task-split thresholds (autotuned for batches): triangle-pass owners with
   // more than te_cta_min upward neighbours (<= 128) and 4-cycle tasks whose
   // 2-hop bound exceeds c4_warp_bound (<= 256) run on a CTA; clique tasks
   // with more than cq_warp_max out-neighbours (<= 64) run on a CTA; 4-cycle
-  // tasks whose bound exceeds c4_big_min count in key-range chunks
+  // tasks whose bound exceeds c4_big_min (<= 3072; GPM_C4_BIG_MIN overrides)
+  // go to the giant-task kernel
   int te_cta_min = 128, c4_warp_bound = 256, cq_warp_max = 64;
-  long long c4_big_min = 4096;
+  long long c4_big_min = 3072;
   int size = 4;  // 3: only the per-edge triangle pass and the degree sums (out[0..1])
 };
 
@@ -64,8 +65,6 @@ struct MotifPlan {
   DevBuf<int64_t> c4_cur;  // per-CTA cursors and list ends of the giant tasks
   int64_t c4_scratch = 0;
   DevBuf<int> te_counters, c4_counters;
-  DevBuf<unsigned> dense;
-  int64_t dense_len = 0;
   CliquePlan k4;
   DevBuf<unsigned long long> acc, out;
 };
