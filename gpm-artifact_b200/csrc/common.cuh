@@ -196,6 +196,7 @@ struct RankPlan;
 struct RankGraph;
 struct LabelCsr;
 struct MotifPlan;
+struct MotifPlan;
 
 }  // namespace gpm
 
@@ -215,6 +216,7 @@ struct gpm_graph {
   gpm::RankGraph *rg = nullptr;  // cached rank-relabelled copy
   gpm::RankPlan *learned = nullptr;  // plan chosen by the attached scheduler
   gpm::LabelCsr *lcsr = nullptr;     // label-partitioned lists (matching)
+  gpm::MotifPlan *motif[2] = {nullptr, nullptr};  // cached motif pipelines (3-, 4-vertex)
   gpm_sched *sched = nullptr;        // learned scheduler (not owned)
   gpm::DevBuf<uint64_t> result; // small device result scratch
   ~gpm_graph();
@@ -230,6 +232,7 @@ void free_tc_plan(TcPlan *p);
 void free_rank_plan(RankPlan *p);
 void free_rank_graph(RankGraph *r);
 void free_label_csr(LabelCsr *p);
+void free_motif_plan(MotifPlan *p);  // motif.cu
 // Drops every cached schedule (after the stored graph changed).
 void drop_plans(gpm_graph *g);
 int num_sms();

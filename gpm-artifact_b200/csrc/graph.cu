@@ -389,6 +389,10 @@ void drop_plans(gpm_graph *g) {
   g->learned = nullptr;
   free_label_csr(g->lcsr);
   g->lcsr = nullptr;
+  for (MotifPlan *&m : g->motif) {
+    free_motif_plan(m);
+    m = nullptr;
+  }
 }
 }  // namespace gpm
 

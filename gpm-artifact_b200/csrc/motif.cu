@@ -357,8 +357,14 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
 // groups of P = 1..32 lanes (P grows as x has fewer neighbours below it); each
 // lane reads four keys per 16-byte load.  Lists far longer than the task's
 // mean are walked by whole warps.
-constexpr int kC4BigThreads = 1024;
-constexpr int kC4BigSmem = 200 * 1024;
+#ifndef GPM_C4_BIG_THREADS
+#define GPM_C4_BIG_THREADS 1024
+#endif
+#ifndef GPM_C4_BIG_KB
+#define GPM_C4_BIG_KB 200
+#endif
+constexpr int kC4BigThreads = GPM_C4_BIG_THREADS;
+constexpr int kC4BigSmem = GPM_C4_BIG_KB * 1024;
 constexpr int kC4BigWords = kC4BigSmem / 4;
 
 struct C4Chunk {
@@ -436,7 +442,7 @@ __device__ __forceinline__ int64_t c4_step(const C4Chunk &q, unsigned *cw, int64
   return jb + rel;
 }
 
-__global__ void __launch_bounds__(kC4BigThreads, 1)
+__global__ void __launch_bounds__(kC4BigThreads, 1024 / kC4BigThreads)
     k_c4_big(const int64_t *__restrict__ roff, const int64_t *__restrict__ split, const int32_t *__restrict__ radj,
              int64_t nnz, const int32_t *__restrict__ gid, const int64_t *__restrict__ gbase,
              const int32_t *__restrict__ tasks, const unsigned long long *__restrict__ task_b, int n_tasks,
@@ -820,6 +826,10 @@ int motif_plan_run_stage(MotifPlan *p, int stage, cudaStream_t st) {
 
 }  // namespace gpm
 
+namespace gpm {
+void free_motif_plan(MotifPlan *p) { delete p; }
+}  // namespace gpm
+
 using namespace gpm;
 
 extern "C" int gpm_motif(gpm_graph *g, int k, uint64_t *out) {
@@ -827,18 +837,28 @@ extern "C" int gpm_motif(gpm_graph *g, int k, uint64_t *out) {
   if (k != 3 && k != 4) return fail(GPM_EUNSUPPORTED, "motif size must be 3 or 4");
   if (g->oriented) return fail(GPM_EINVAL, "motif counting needs the symmetric (unoriented) graph");
   GPM_TRY(ensure_rank_graph(g, 0));
-  MotifInput in;
-  in.n = g->n;
-  in.nnz = g->nnz;
-  in.roff = g->rg->roff.p;
-  in.radj = g->rg->radj.p;
-  in.max_graph_n = g->n;
-  in.size = k;
-  MotifPlan plan;
-  GPM_TRY(motif_plan_build(in, &plan, 0));
-  GPM_TRY(motif_plan_run(&plan, 0));
+  // the pipeline (task queues, scratch) is built on the first call of each
+  // size and kept with the graph, so later calls only launch
+  MotifPlan *&plan = g->motif[k - 3];
+  if (!plan) {
+    MotifInput in;
+    in.n = g->n;
+    in.nnz = g->nnz;
+    in.roff = g->rg->roff.p;
+    in.radj = g->rg->radj.p;
+    in.max_graph_n = g->n;
+    in.size = k;
+    MotifPlan *p = new MotifPlan();
+    const int s = motif_plan_build(in, p, 0);
+    if (s != GPM_OK) {
+      delete p;
+      return s;
+    }
+    plan = p;
+  }
+  GPM_TRY(motif_plan_run(plan, 0));
   unsigned long long h[8];
-  GPM_CUDA(cudaMemcpy(h, plan.out.p, sizeof h, cudaMemcpyDeviceToHost));
+  GPM_CUDA(cudaMemcpy(h, plan->out.p, sizeof h, cudaMemcpyDeviceToHost));
   if (k == 3) {
     out[0] = h[0];
     out[1] = h[1];

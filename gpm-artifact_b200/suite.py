@@ -1,12 +1,14 @@
 """Measurements of the engine's other workloads, each beside its plain path.
 
-    python gpm-artifact_b200/suite.py [--only er,clique,motif,match,batch] [--quick]
+    python gpm-artifact_b200/suite.py [--only er,clique,motif,motifcl,match,batch] [--quick]
 
 Prints one JSON line per workload:
   er      triangle count, Erdos-Renyi G(16384, 131072 draws), degree-oriented
   clique  4- and 5-cliques, R-MAT scale 20 (ef 16): local-bitset kernel vs the
           edge-centric kernel shaped like the reference's clique_k_edge_warp
   motif   all 3- and 4-vertex motifs of R-MAT scale 18 (ef 16, seed 1)
+  motifcl all 3- and 4-vertex motifs of a Chung-Lu graph (n 200,000, exponent
+          2.18, mean degree 62): hub-dominated 4-cycles
   match   labelled matching with sub_ceci semantics, R-MAT with 8 Zipf(1.2)
           labels, five queries (triangle, 4-cycle, diamond, house, 6-vertex
           pyramid = apex over a 5-cycle) found by seeded random walks on the
@@ -15,8 +17,9 @@ Prints one JSON line per workload:
           [1e3, 1e6], exponent U[2.1, 2.8], mean degree U[8, 64]): one union,
           one launch per stage, CUDA-graph replay, autotuned -- against one
           gpm_motif call per graph
-Times are CUDA-event or synchronised wall times of the counting calls; graph
-generation and host copies are outside them unless named.
+Times are medians of synchronised wall times of repeated counting calls
+(first calls, which include relabelling and planning, are single samples);
+graph generation and host copies are outside them unless named.
 """
 from __future__ import annotations
 
@@ -41,13 +44,17 @@ SHAPES = {
 
 
 def timed(fn, reps=1):
+    """Result and median wall time of `reps` synchronised calls (medians:
+    the GPUs and hosts these runs share see other users' work)."""
     import torch
-    torch.cuda.synchronize()
-    t = time.perf_counter()
+    ts = []
     for _ in range(reps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
         r = fn()
-    torch.cuda.synchronize()
-    return r, (time.perf_counter() - t) / reps
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t)
+    return r, float(np.median(ts))
 
 
 def walk_query(off, idx, labels, shape, rng, tries=2000):
@@ -105,8 +112,12 @@ def run_er():
     res = {}
     for name, v in (("bitmap", gpm.TC_BITMAP), ("hash", gpm.TC_HASH), ("bsearch", gpm.TC_BSEARCH)):
         g.tc_async(v, sp, out.data_ptr())
-        _, t = timed(lambda: g.tc_async(v, sp, out.data_ptr()), 20)
-        res[name] = t * 1e3
+
+        def burst():  # 20 counts queued back to back on the stream
+            for _ in range(20):
+                g.tc_async(v, sp, out.data_ptr())
+        _, t = timed(burst, 5)
+        res[name] = t / 20 * 1e3
     m = g.info().nnz
     return {"workload": "tc_er_16384_131072", "triangles": int(out.item()), "m": m,
             "ms_per_count": res, "teps_bitmap": m / (res["bitmap"] / 1e3)}
@@ -117,8 +128,8 @@ def run_clique(scale):
     res = {"workload": f"clique_rmat{scale}_ef16"}
     for k in (4, 5):
         _, t0 = timed(lambda: g.clique(k))  # first call: relabel (k = 4 only) and plan
-        c, t = timed(lambda: g.clique(k))
-        c2, t2 = timed(lambda: g.clique(k, edge_centric=True))
+        c, t = timed(lambda: g.clique(k), 5)
+        c2, t2 = timed(lambda: g.clique(k, edge_centric=True), 3)
         assert c == c2, (k, c, c2)
         res[f"k{k}"] = {"cliques": c, "ms_first_call": t0 * 1e3, "ms_bitset": t * 1e3, "ms_edge_centric": t2 * 1e3,
                         "cliques_per_s": c / t, "speedup": t2 / t}
@@ -129,13 +140,25 @@ def run_motif(scale):
     """All 3- and 4-vertex motifs of one R-MAT graph (edge factor 16, seed
     1): first call (relabel and plan included) and repeated calls."""
     g = gpm.Graph.rmat(scale, 16, seed=1)
+    return motif_result(g, f"motif_rmat{scale}_ef16")
+
+
+def motif_result(g, name):
     m4, t_first = timed(lambda: g.motif(4))
-    m4b, t = timed(lambda: g.motif(4), 3)
+    m4b, t = timed(lambda: g.motif(4), 7)
     assert m4.tolist() == m4b.tolist()
-    m3, t3 = timed(lambda: g.motif(3), 3)
-    return {"workload": f"motif_rmat{scale}_ef16", "m": g.info().nnz // 2, "motif4": [int(x) for x in m4],
+    m3, t3 = timed(lambda: g.motif(3), 7)
+    return {"workload": name, "m": g.info().nnz // 2, "motif4": [int(x) for x in m4],
             "motif3": [int(x) for x in m3], "s_motif4_first": t_first, "s_motif4": t, "s_motif3": t3,
             "instances_per_s": float(m4.sum()) / t}
+
+
+def run_motif_chung_lu():
+    """All 3- and 4-vertex motifs of one heavy-tailed Chung-Lu graph
+    (n = 200,000, exponent 2.18, mean degree 62, seed 11): 4-cycles are
+    dominated by hub tasks with ~10^5-10^6 distinct 2-hop endpoints."""
+    n, s, d = gpm.gen_chung_lu(200000, 2.18, 62.0, seed=11)
+    return motif_result(gpm.Graph.from_edges(n, s, d), "motif_chunglu_200000_g2.18_d62")
 
 
 def run_match(scale, seed=3):
@@ -220,7 +243,7 @@ def run_batch(count, nmax):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", default="er,clique,motif,match,batch")
+    ap.add_argument("--only", default="er,clique,motif,motifcl,match,batch")
     ap.add_argument("--quick", action="store_true", help="smaller sizes for a smoke run")
     ap.add_argument("--match-scales", default="", help="e.g. 16,18,20,21: the labelled workload at growing scales")
     ap.add_argument("--match-budget", type=float, default=240.0, help="seconds a query may take at its last scale x 8")
@@ -232,6 +255,8 @@ def main():
         print(json.dumps(run_clique(16 if a.quick else 20)), flush=True)
     if "motif" in todo:
         print(json.dumps(run_motif(14 if a.quick else 18)), flush=True)
+    if "motifcl" in todo:
+        print(json.dumps(run_motif_chung_lu()), flush=True)
     if "match" in todo:
         if a.match_scales:
             print(json.dumps(run_match_scales([int(x) for x in a.match_scales.split(",")], a.match_budget)),

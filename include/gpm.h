@@ -13,7 +13,11 @@
  *     reference's binary searches, src/graph/search.cuh:20-87, are only
  *     defined on such lists);
  *   - "stream" arguments are a cudaStream_t passed as void* (NULL = the
- *     legacy default stream).  Synchronous calls block on that stream.
+ *     legacy default stream).  Synchronous calls block on that stream;
+ *   - a graph handle keeps what its first calls build (the rank-relabelled
+ *     copy, task queues and scratch of each count), so repeated counts on it
+ *     only launch; calls on one handle from several host threads at once
+ *     race on those caches.
  */
 #ifndef GPM_H
 #define GPM_H
@@ -220,7 +224,8 @@ int gpm_clique_ex(gpm_graph *g, int k, int variant, uint64_t *out);
 /* Motif counting on a symmetric graph.  k = 3: out[0] = induced 2-paths,
  * out[1] = triangles.  k = 4: out[0..5] = 3-star, 4-path, tailed triangle,
  * 4-cycle, diamond, 4-clique -- the counter order of Motif4_G2Miner
- * (src/gpu_kernels/G2Miner_kernels.cuh:473-548). */
+ * (src/gpu_kernels/G2Miner_kernels.cuh:473-548).  The first call of each k
+ * builds the pipeline's task queues and scratch and keeps them with g. */
 int gpm_motif(gpm_graph *g, int k, uint64_t *out);
 
 /* G2MinerSolver / PatternSolver (src/G2MinerSolver.cuh:17-176,

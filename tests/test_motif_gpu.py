@@ -138,3 +138,17 @@ def test_giant_tasks_many_chunks_and_wide_counters():
     assert r[0].tolist() == r[2].tolist()
     soff, sidx = sym(sn, ss, sd)
     assert r[0, 2:].tolist() == orc.motif4(soff, sidx).tolist()
+
+
+def test_cached_pipelines_repeat_exactly():
+    """The first call of each motif size keeps its pipeline with the graph;
+    later calls, interleaved with the other size, only relaunch it and give
+    the same counts."""
+    n, s, d = gpm.gen_chung_lu(5000, 2.2, 20.0, seed=21)
+    off, idx = sym(n, s, d)
+    want4 = orc.motif4(off, idx).tolist()
+    want3 = orc.motif3(off, idx, orc.tc(*orc.orient(off, idx))).tolist()
+    g = gpm.Graph.from_edges(n, s, d)
+    for _ in range(3):
+        assert g.motif(4).tolist() == want4
+        assert g.motif(3).tolist() == want3
