@@ -457,12 +457,28 @@ int clique_run_upward(int64_t n, const int64_t *roff, const int32_t *radj, int m
   return GPM_OK;
 }
 
+void free_clique_plan(CliquePlan *p) { delete p; }
+
 int clique_launch(gpm_graph *g, int k, cudaStream_t st, unsigned long long *d_out, bool edge_centric = false) {
   GPM_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
   if (g->nnz == 0) return GPM_OK;
   GPM_TRY(ensure_rank_graph(g, st));
-  if (!edge_centric && g->rg->upward && g->max_deg <= kCqCtaMax)
-    return clique_run_upward(g->n, g->rg->roff.p, g->rg->radj.p, g->max_deg, k, nullptr, d_out, 0, 0, st);
+  if (!edge_centric && g->rg->upward && g->max_deg <= kCqCtaMax) {
+    // the schedule (task queues, per-CTA bitset slabs) is built on the first
+    // call for this k and kept with the graph
+    CliquePlan *&p = g->clique[k];
+    if (!p) {
+      CliquePlan *q = new CliquePlan();
+      const int s = clique_plan_build(q, g->n, g->rg->roff.p, g->rg->radj.p, g->max_deg, k, nullptr, d_out, 0, 0, st);
+      if (s != GPM_OK) {
+        delete q;
+        return s;
+      }
+      p = q;
+    }
+    p->acc = d_out;
+    return clique_plan_run(p, st);
+  }
   // edge-centric path on the stored graph
   GPM_TRY(ensure_src(g, st));
   int grid = num_sms() * 8;

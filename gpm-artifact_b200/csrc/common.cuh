@@ -196,6 +196,7 @@ struct RankPlan;
 struct RankGraph;
 struct LabelCsr;
 struct MotifPlan;
+struct CliquePlan;
 struct MotifPlan;
 
 }  // namespace gpm
@@ -217,6 +218,7 @@ struct gpm_graph {
   gpm::RankPlan *learned = nullptr;  // plan chosen by the attached scheduler
   gpm::LabelCsr *lcsr = nullptr;     // label-partitioned lists (matching)
   gpm::MotifPlan *motif[2] = {nullptr, nullptr};  // cached motif pipelines (3-, 4-vertex)
+  gpm::CliquePlan *clique[9] = {};                // cached k-clique schedules, by k
   gpm_sched *sched = nullptr;        // learned scheduler (not owned)
   gpm::DevBuf<uint64_t> result; // small device result scratch
   ~gpm_graph();
@@ -233,6 +235,7 @@ void free_rank_plan(RankPlan *p);
 void free_rank_graph(RankGraph *r);
 void free_label_csr(LabelCsr *p);
 void free_motif_plan(MotifPlan *p);  // motif.cu
+void free_clique_plan(CliquePlan *p);  // clique.cu
 // Drops every cached schedule (after the stored graph changed).
 void drop_plans(gpm_graph *g);
 int num_sms();

@@ -393,6 +393,10 @@ void drop_plans(gpm_graph *g) {
     free_motif_plan(m);
     m = nullptr;
   }
+  for (CliquePlan *&c : g->clique) {
+    free_clique_plan(c);
+    c = nullptr;
+  }
 }
 }  // namespace gpm
 

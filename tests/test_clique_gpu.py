@@ -85,3 +85,17 @@ def test_bad_k():
         g.clique(2)
     with pytest.raises(gpm.GpmError):
         g.clique(9)
+
+
+def test_cached_schedules_repeat_exactly():
+    """Each k's schedule is built on its first call and kept with the graph;
+    interleaved repeated calls (and the edge-centric kernel between them)
+    give the oracle's counts every time."""
+    n, s, d = gpm.gen_rmat(13, 16, seed=23)
+    off, idx, doff, didx = dag(n, s, d)
+    want = {k: orc.clique(doff, didx, k) for k in (3, 4, 5)}
+    g = gpm.Graph.rmat(13, 16, seed=23).orient()
+    for _ in range(3):
+        for k in (5, 3, 4):
+            assert g.clique(k) == want[k], k
+        assert g.clique(4, edge_centric=True) == want[4]
