@@ -159,7 +159,10 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restri
           int32_t x = 0;
           if (i < e) {
             x = __ldg(seg + i);
-            ok = labels[x] == lab && off[x + 1] - off[x] >= q.mindeg[depth];
+            // a label segment holds only that label (L > 0); at the last
+            // level every query edge of the vertex is a back-edge checked
+            // below, so the degree bound prunes nothing there
+            ok = (L > 0 || labels[x] == lab) && (last || off[x + 1] - off[x] >= q.mindeg[depth]);
             for (int j = 0; ok && j < depth; ++j) ok = emb[j] != x;
             uint32_t bm = nb;
             while (ok && bm) {
