@@ -233,6 +233,14 @@ __device__ __forceinline__ int c4_slot(int2 *tab, int32_t y) {
   return -1;
 }
 
+// Empties a (key, count) table of `slots` entries (16-byte aligned, slots
+// even) with 16-byte stores.  Counts need no scan before it: every increment
+// adds the counter's old value to the task's sum (C(c+1,2) - C(c,2) = c).
+__device__ __forceinline__ void c4_reset(int2 *tab, int slots, int t, int nt) {
+  uint4 *v = reinterpret_cast<uint4 *>(tab);
+  for (int i = t; i < slots / 2; i += nt) v[i] = make_uint4(0xffffffffu, 0u, 0xffffffffu, 0u);
+}
+
 __global__ void k_c4_tasks(int64_t n, const int64_t *__restrict__ roff, const int64_t *__restrict__ split,
                            const int32_t *__restrict__ radj, int warp_bound, long long big_min,
                            int32_t *__restrict__ cta_tasks, int32_t *__restrict__ warp_tasks,
@@ -269,7 +277,7 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
                                             const int64_t *__restrict__ gbase, const int32_t *__restrict__ cta_tasks,
                                             int n_cta, const int32_t *__restrict__ warp_tasks, int n_warp,
                                             int *__restrict__ counters, unsigned long long *__restrict__ acc) {
-  __shared__ int2 c4sm[8 * kC4WarpCap];
+  __shared__ __align__(16) int2 c4sm[8 * kC4WarpCap];
   __shared__ int s_task;
   const unsigned lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;
@@ -284,28 +292,25 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
     const int32_t x = cta_tasks[t];
     const int g = graph_of(gid, x);
     const int64_t a0 = roff[x], a1 = split[x];
-    for (int i = threadIdx.x; i < kC4CtaSlots; i += blockDim.x) c4sm[i] = make_int2(-1, 0);
+    c4_reset(c4sm, kC4CtaSlots, threadIdx.x, blockDim.x);
     __syncthreads();
+    unsigned long long c = 0;
     for (int64_t k = a0 + wid; k < a1; k += 8) {
       int32_t a = radj[k];
       for (int64_t j = roff[a] + lane; j < roff[a + 1]; j += 32) {
         int32_t y = __ldg(radj + j);
         if (y >= x) break;
         const int h = c4_slot(c4sm, y);
-        if (h >= 0) atomicAdd(&c4sm[h].y, 1);
+        if (h >= 0) c += (unsigned long long)atomicAdd(&c4sm[h].y, 1);
       }
     }
-    __syncthreads();
-    unsigned long long c = 0;
-    for (int i = threadIdx.x; i < kC4CtaSlots; i += blockDim.x)
-      if (c4sm[i].x >= 0) c += choose2((unsigned long long)c4sm[i].y);
     c = warp_sum(c);
     if (lane == 0 && c) atomicAdd(&acc[8 * g + 6], c);
     __syncthreads();
   }
   // tail tasks: shared-memory (key, count) table per warp
   int2 *tab = c4sm + wid * kC4WarpCap;
-  for (int i = lane; i < kC4WarpCap; i += 32) tab[i] = make_int2(-1, 0);
+  c4_reset(tab, kC4WarpCap, lane, 32);
   __syncwarp();
   while (true) {
     int t = 0;
@@ -313,6 +318,7 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= n_warp) break;
     const int32_t x = warp_tasks[t];
+    unsigned long long c = 0;
     for (int64_t k = roff[x]; k < split[x]; ++k) {
       int32_t a = radj[k];
       for (int64_t j = roff[a] + lane; j < roff[a + 1]; j += 32) {
@@ -324,18 +330,11 @@ __global__ void __launch_bounds__(256) k_c4(const int64_t *__restrict__ roff, co
           if (prev == -1 || prev == y) break;
           h = (h + 1) & (kC4WarpCap - 1);
         }
-        atomicAdd(&tab[h].y, 1);
+        c += (unsigned long long)atomicAdd(&tab[h].y, 1);
       }
     }
     __syncwarp();
-    unsigned long long c = 0;
-    for (int i = lane; i < kC4WarpCap; i += 32) {
-      int2 s = tab[i];
-      if (s.x >= 0) {
-        c += choose2((unsigned long long)s.y);
-        tab[i] = make_int2(-1, 0);
-      }
-    }
+    c4_reset(tab, kC4WarpCap, lane, 32);
     __syncwarp();
     c = warp_sum(c);
     if (lane == 0 && c) atomicAdd(&acc[8 * graph_of(gid, x) + 6], c);
