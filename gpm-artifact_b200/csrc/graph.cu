@@ -5,6 +5,7 @@
 // HBM layout of a graph: off[n+1] (int64), adj[nnz] (int32), lists sorted
 // ascending, optional labels[n] (int32) and a lazily built COO source array
 // src[nnz] (int32) for edge-parallel kernels.
+#include <atomic>
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -16,14 +17,16 @@
 namespace gpm {
 
 int num_sms() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return sms;
+  // per device: a process may drive GPUs with different SM counts
+  constexpr int kDevs = 64;
+  static std::atomic<int> sms[kDevs];
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < kDevs && (v = sms[dev].load(std::memory_order_relaxed)) > 0) return v;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  if (v <= 0) v = 148;
+  if (dev >= 0 && dev < kDevs) sms[dev].store(v, std::memory_order_relaxed);
+  return v;
 }
 
 static constexpr uint64_t kSentinel = ~0ull;
@@ -580,6 +583,13 @@ int gpm_graph_relabel(gpm_graph *g) {
   GPM_TRY(relabel_device(g, 0));
   GPM_TRY(compute_max_degree(g, 0));
   GPM_CUDA(cudaDeviceSynchronize());
+  return GPM_OK;
+}
+
+int gpm_graph_drop_plans(gpm_graph *g) {
+  if (!g) return fail(GPM_EINVAL, "NULL graph");
+  GPM_CUDA(cudaDeviceSynchronize());  // no kernel may still read what is freed
+  drop_plans(g);
   return GPM_OK;
 }
 

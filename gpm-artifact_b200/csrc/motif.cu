@@ -217,6 +217,7 @@ constexpr int kC4CtaSlots = 8 * kC4WarpCap;  // a hub task's shared table: the 8
 // k_c4_big), so at most that many distinct keys meet kC4CtaSlots slots: the
 // table never fills and every probe sequence ends.
 constexpr long long kC4HubMax = kC4CtaSlots * 3 / 4;
+static_assert(kC4HubMax < kC4CtaSlots, "a hub task's keys must leave its table a free slot: c4_slot never fails");
 
 // Slot of y in a hub task's shared table, found or newly claimed.
 __device__ __forceinline__ int c4_slot(int2 *tab, int32_t y) {
@@ -722,6 +723,8 @@ int motif_plan_build(const MotifInput &in, MotifPlan *p, cudaStream_t st) {
       long long big_min = in.c4_big_min;
       if (const char *e = getenv("GPM_C4_BIG_MIN")) big_min = atoll(e);
       big_min = std::min(std::max<long long>(big_min, (long long)wb), kC4HubMax);
+      // hub tasks (bound <= big_min) must fit c4_slot's table, or they would drop wedges
+      if (big_min > kC4HubMax) return fail(GPM_EINVAL, "4-cycle hub bound above the hub table");
       k_c4_tasks<<<grid_for(n * 32), 256, 0, st>>>(n, roff, p->split.p, radj, wb, big_min,
                                                    p->c4_ct.p, p->c4_wt.p, bt.p, bb.p, sizes.p + 2);
     }

@@ -488,9 +488,17 @@ static __device__ __align__(256) int32_t g_noalloc_scratch[kNoAllocHeader + 2 * 
 // so the address is looked up once per device and kept here.
 constexpr int kNoAllocMaxDevices = 64;
 static int32_t *g_noalloc_ptr[kNoAllocMaxDevices];
+static int g_noalloc_grid[kNoAllocMaxDevices];  // resident CTAs of k_tc_hash_noalloc x SMs, per device
 static std::mutex g_noalloc_mu;
 
-static int noalloc_scratch(int32_t **out) {
+__global__ void __launch_bounds__(256) k_tc_hash_noalloc(const int64_t *__restrict__ off,
+                                                         const int32_t *__restrict__ adj,
+                                                         const int32_t *__restrict__ cta_tasks,
+                                                         const int32_t *__restrict__ warp_tasks,
+                                                         const int *__restrict__ sizes, int *__restrict__ counters,
+                                                         unsigned long long *__restrict__ out);
+
+static int noalloc_scratch(int32_t **out, int *grid) {
   int dev = 0;
   GPM_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(GPM_EUNSUPPORTED, "device index above 63");
@@ -502,9 +510,13 @@ static int noalloc_scratch(int32_t **out) {
       cudaGetLastError();
       return fail(GPM_ECUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
     }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_hash_noalloc, 256, TC_SMEM);
+    g_noalloc_grid[dev] = std::max(1, per_sm) * num_sms();
     g_noalloc_ptr[dev] = static_cast<int32_t *>(p);
   }
   *out = g_noalloc_ptr[dev];
+  *grid = g_noalloc_grid[dev];
   return GPM_OK;
 }
 
@@ -552,7 +564,8 @@ extern "C" int gpm_tc_csr_noalloc(int64_t n, const int64_t *d_offsets, const int
                                 " vertices exceed the 1048576-vertex limit of the no-allocation entry point");
   cudaStream_t st = (cudaStream_t)stream;
   int32_t *scratch = nullptr;
-  GPM_TRY(noalloc_scratch(&scratch));
+  int hash_grid = 0;
+  GPM_TRY(noalloc_scratch(&scratch, &hash_grid));
   int *sizes = scratch, *counters = scratch + 16;
   int32_t *cta_tasks = scratch + kNoAllocHeader, *warp_tasks = cta_tasks + kNoAllocMaxVertices;
   GPM_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int32_t) * kNoAllocHeader, st));
@@ -562,12 +575,7 @@ extern "C" int gpm_tc_csr_noalloc(int64_t n, const int64_t *d_offsets, const int
   int grid = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8);
   k_tc_split<<<grid, 256, 0, st>>>(n, d_offsets, 2, 101, cta_tasks, warp_tasks, sizes);
   GPM_LAUNCH_CHECK();
-  static int per_sm = 0;
-  if (!per_sm) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_hash_noalloc, 256, TC_SMEM);
-    if (per_sm < 1) per_sm = 1;
-  }
-  k_tc_hash_noalloc<<<per_sm * num_sms(), 256, TC_SMEM, st>>>(d_offsets, d_indices, cta_tasks, warp_tasks, sizes,
+  k_tc_hash_noalloc<<<hash_grid, 256, TC_SMEM, st>>>(d_offsets, d_indices, cta_tasks, warp_tasks, sizes,
                                                               counters, (unsigned long long *)d_out);
   GPM_LAUNCH_CHECK();
   return GPM_OK;

@@ -64,6 +64,7 @@ _SIGS = {
     "gpm_graph_set_labels": ([_P, _P], c_int),
     "gpm_graph_orient": ([_P, c_int], c_int),
     "gpm_graph_work": ([_P, POINTER(c_uint64), POINTER(c_uint64)], c_int),
+    "gpm_graph_drop_plans": ([_P], c_int),
     "gpm_tc": ([_P, c_int, POINTER(c_uint64)], c_int),
     "gpm_tc_async": ([_P, c_int, _P, _P], c_int),
     "gpm_tc_host_csr": ([c_int64, _P, _P, c_int, _P, POINTER(c_uint64)], c_int),
@@ -238,6 +239,23 @@ class Graph:
         return cls(h)
 
     @classmethod
+    def from_csr_ptrs(cls, n, off_ptr, idx_ptr, labels_ptr=None):
+        """from_csr on raw host pointers (e.g. pinned buffers)."""
+        h = c_void_p()
+        check(lib.gpm_graph_create_csr(n, c_void_p(off_ptr), c_void_p(idx_ptr),
+                                       c_void_p(labels_ptr) if labels_ptr else None, ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_edge_ptrs(cls, n, m, src_ptr, dst_ptr, labels_ptr=None, symmetrize=True):
+        """from_edges on raw host pointers (e.g. pinned buffers)."""
+        h = c_void_p()
+        check(lib.gpm_graph_create(n, m, c_void_p(src_ptr), c_void_p(dst_ptr),
+                                   c_void_p(labels_ptr) if labels_ptr else None, SYMMETRIZE if symmetrize else 0,
+                                   ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
     def generate(cls, kind, p0, p1=0, a=0.0, b=0.0, c=0.0, seed=1):
         h = c_void_p()
         check(lib.gpm_graph_generate(kind, p0, p1, a, b, c, seed, ctypes.byref(h)))
@@ -272,6 +290,11 @@ class Graph:
 
     def orient(self, relabel=False):
         check(lib.gpm_graph_orient(self.h, 1 if relabel else 0))
+        return self
+
+    def drop_plans(self):
+        """Frees the schedules earlier counts cached with this graph."""
+        check(lib.gpm_graph_drop_plans(self.h))
         return self
 
     def work(self):
@@ -427,6 +450,16 @@ class Batch:
         dst = _i32(np.concatenate([x[2] for x in members]) if len(members) else [])
         h = c_void_p()
         check(lib.gpm_batch_create(len(members), _ptr(n), _ptr(m), _ptr(src), _ptr(dst), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_edge_ptrs(cls, n, m, src_ptr, dst_ptr):
+        """from_edges with member sizes n[], m[] and all members' edges back
+        to back behind raw host pointers (e.g. pinned buffers)."""
+        n = np.ascontiguousarray(n, np.int64)
+        m = np.ascontiguousarray(m, np.int64)
+        h = c_void_p()
+        check(lib.gpm_batch_create(len(n), _ptr(n), _ptr(m), c_void_p(src_ptr), c_void_p(dst_ptr), ctypes.byref(h)))
         return cls(h)
 
     @classmethod

@@ -34,13 +34,7 @@ import numpy as np
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import gpm  # noqa: E402
 
-SHAPES = {
-    "triangle": (3, [(0, 1), (1, 2), (2, 0)]),
-    "cycle4": (4, [(0, 1), (1, 2), (2, 3), (3, 0)]),
-    "diamond": (4, [(0, 1), (0, 2), (0, 3), (1, 2), (2, 3)]),
-    "house": (5, [(0, 1), (0, 4), (1, 2), (1, 4), (2, 3), (3, 4)]),
-    "pyramid6": (6, [(0, 1), (0, 2), (0, 3), (0, 4), (0, 5), (1, 2), (2, 3), (3, 4), (4, 5), (5, 1)]),
-}
+from workloads import SHAPES, batch_members, walk_query  # noqa: E402
 
 
 def timed(fn, reps=1):
@@ -55,52 +49,6 @@ def timed(fn, reps=1):
         torch.cuda.synchronize()
         ts.append(time.perf_counter() - t)
     return r, float(np.median(ts))
-
-
-def walk_query(off, idx, labels, shape, rng, tries=2000):
-    """An embedding of `shape` found by a seeded randomised walk (depth-first,
-    random neighbour order); returns the walked vertices' labels."""
-    k, edges = shape
-    adj = [set() for _ in range(k)]
-    for a, b in edges:
-        adj[a].add(b)
-        adj[b].add(a)
-    n = len(off) - 1
-    deg = np.diff(off)
-
-    def nbrs(v):
-        return idx[off[v]:off[v + 1]]
-
-    def has(a, b):
-        lst = nbrs(a)
-        i = np.searchsorted(lst, b)
-        return i < len(lst) and lst[i] == b
-
-    for _ in range(tries):
-        start = int(rng.integers(n))
-        if deg[start] < len(adj[0]):
-            continue
-        emb = [start]
-
-        def extend(i):
-            if i == k:
-                return True
-            parent = next(j for j in range(i) if j in adj[i])
-            cand = nbrs(emb[parent])
-            for v in rng.permutation(cand)[:64]:
-                v = int(v)
-                if v in emb or deg[v] < len(adj[i]):
-                    continue
-                if all(has(emb[j], v) for j in range(i) if j in adj[i]):
-                    emb.append(v)
-                    if extend(i + 1):
-                        return True
-                    emb.pop()
-            return False
-
-        if extend(1):
-            return labels[np.array(emb)]
-    raise RuntimeError("no embedding found")
 
 
 def run_er():
@@ -206,13 +154,6 @@ def run_match_scales(scales, budget_s, seed=3):
         g.close()
     return res
 
-
-def batch_members(count, nmax, seed=5):
-    rng = np.random.default_rng(seed)
-    n = np.exp(rng.uniform(np.log(1e3), np.log(nmax), count)).astype(np.int64)
-    gam = rng.uniform(2.1, 2.8, count)
-    md = rng.uniform(8, 64, count)
-    return n, gam, md
 
 
 def run_batch(count, nmax):

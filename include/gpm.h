@@ -168,6 +168,11 @@ int gpm_graph_set_labels(gpm_graph *g, const int32_t *labels);
 int gpm_graph_orient(gpm_graph *g, int relabel);
 /* Graph::SortCSRGraph (graph.h:206-252) alone, on the current lists. */
 int gpm_graph_relabel(gpm_graph *g);
+/* Frees what earlier counts cached with g (the rank-relabelled copy, task
+ * queues, pipelines, label partition), keeping the graph itself; the next
+ * count builds them again.  No reference counterpart: the reference keeps no
+ * schedules between calls (and leaks its scratch, src/TCSolver.cuh:72,105). */
+int gpm_graph_drop_plans(gpm_graph *g);
 /* Algorithmic work figures of the (oriented) graph: *wedge_work =
  * sum over stored u->v of deg(v); *pair_work = sum over u->v of
  * (deg(u) + deg(v)). */
@@ -200,9 +205,10 @@ int gpm_tc_plan_stats(gpm_graph *g, uint64_t *stats);
  * cannot call cudaMalloc (a framework owning all device memory through its
  * own pool, services that forbid allocation after start-up, code that must
  * avoid the implicit synchronisation of allocation).  d_offsets[n+1] (int64)
- * and d_indices (int32, sorted lists) are the caller's device arrays; the
- * count (sum over stored u->v of |N(u) & N(v)|, the triangle count of a
- * degree-oriented graph) is written to the caller's device uint64 d_out on
+ * and d_indices (int32, sorted lists, every id < n) are the caller's device
+ * arrays, nothing of them is checked (ids outside [0, n) read out of bounds);
+ * the count (sum over stored u->v of |N(u) & N(v)|, the triangle count when
+ * the CSR is a degree-oriented DAG, which the caller orients) is written to the caller's device uint64 d_out on
  * `stream` without host synchronisation.  Scratch lives in a fixed 8 MiB
  * array inside the library: at most 1,048,576 vertices (larger n is
  * rejected with GPM_EINVAL); calls that overlap on the GPU race on that

@@ -18,6 +18,7 @@
  */
 #include "gpm_oracle.h"
 
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -188,6 +189,13 @@ static uint64_t clique_rec(const int64_t *off, const int32_t *idx, const int32_t
 }
 
 uint64_t orc_clique(int64_t n, const int64_t *doff, const int32_t *didx, int k, int threads) {
+  return orc_clique_tasks(n, doff, didx, k, NULL, threads);
+}
+
+/* orc_clique over the tasks (first DAG vertices) u with keep[u] != 0, or all
+ * of them when keep is NULL: a bounded sample for the CPU baseline. */
+uint64_t orc_clique_tasks(int64_t n, const int64_t *doff, const int32_t *didx, int k, const uint8_t *keep,
+                          int threads) {
   const int64_t *off = doff;
   const int32_t *idx = didx;
   uint64_t total = 0;
@@ -202,6 +210,7 @@ uint64_t orc_clique(int64_t n, const int64_t *doff, const int32_t *didx, int k, 
 #pragma omp for schedule(dynamic, 64)
     for (u = 0; u < n; u++) {
       int64_t e;
+      if (keep && !keep[u]) continue;
       for (e = off[u]; e < off[u + 1]; e++) {
         int32_t v = idx[e];
         /* level-2 list W = N+(u) & N+(v), as clique_4_edge_warp does */
@@ -226,6 +235,13 @@ static int64_t max_degree(int64_t n, const int64_t *off) {
 
 void orc_motif4_g2miner(int64_t n, const int64_t *off, const int32_t *idx,
                         uint64_t *out, int threads) {
+  orc_motif4_tasks(n, off, idx, NULL, out, threads);
+}
+
+/* orc_motif4_g2miner over the edge tasks of the vertices v0 with keep[v0] != 0
+ * (all when keep is NULL): a bounded sample for the CPU baseline. */
+void orc_motif4_tasks(int64_t n, const int64_t *off, const int32_t *idx, const uint8_t *keep,
+                      uint64_t *out, int threads) {
   uint64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0;
   int64_t maxd = max_degree(n, off), v0;
   set_threads(threads);
@@ -236,6 +252,7 @@ void orc_motif4_g2miner(int64_t n, const int64_t *off, const int32_t *idx,
 #pragma omp for schedule(dynamic, 64)
     for (v0 = 0; v0 < n; v0++) {
       int64_t e, i, j;
+      if (keep && !keep[v0]) continue;
       for (e = off[v0]; e < off[v0 + 1]; e++) {
         int32_t v1 = idx[e];
         int64_t n0, n1;
@@ -787,4 +804,180 @@ uint64_t orc_tc_weighted(int64_t n, const int64_t *doff, const int32_t *didx, co
     free(mark);
   }
   return total;
+}
+
+/* ------------------------------------------------------------------ */
+/* seeded synthetic generators                                         */
+/* ------------------------------------------------------------------ */
+/* The engine draws every synthetic graph from a counter-based generator
+ * (splitmix64's finaliser applied to (seed, stream, index)), so edge i of a
+ * seed is the same on any thread.  These are the same draws written again in
+ * C, so that a harness which must not load the engine -- the CPU reference
+ * arm of bench.py, fixture scripts -- builds the very same graphs.  A CPU
+ * test checks them against the engine's host generators edge for edge. */
+static uint64_t g_mix(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+static uint64_t g_draw(uint64_t seed, uint64_t stream, uint64_t i) {
+  return g_mix(g_mix(seed ^ (stream * 0xD1B54A32D192ED03ull)) ^ i);
+}
+static double g_unit(uint64_t r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
+static uint32_t g_below(uint64_t r, uint64_t n) { return (uint32_t)(((r >> 32) * n) >> 32); }
+
+/* R-MAT: edge i descends `scale` levels, level l choosing quadrant a / b / c /
+ * d (row bit, column bit) = (0,0) / (0,1) / (1,0) / (1,1) from draw stream 1+l. */
+void orc_gen_rmat(int scale, int64_t m, double a, double b, double c, uint64_t seed, int32_t *src,
+                  int32_t *dst, int threads) {
+  int64_t i;
+  const double ab = a + b, abc = a + b + c;
+  set_threads(threads);
+#pragma omp parallel for schedule(static)
+  for (i = 0; i < m; i++) {
+    uint32_t x = 0, y = 0;
+    int l;
+    for (l = 0; l < scale; l++) {
+      const double r = g_unit(g_draw(seed, (uint64_t)(1 + l), (uint64_t)i));
+      const uint32_t bx = r >= ab, by = (r >= a && r < ab) || r >= abc;
+      x = (x << 1) | bx;
+      y = (y << 1) | by;
+    }
+    src[i] = (int32_t)x;
+    dst[i] = (int32_t)y;
+  }
+}
+
+/* Erdos-Renyi G(n, m draws): endpoints uniform from streams 101 and 102. */
+void orc_gen_er(int64_t n, int64_t m, uint64_t seed, int32_t *src, int32_t *dst, int threads) {
+  int64_t i;
+  set_threads(threads);
+#pragma omp parallel for schedule(static)
+  for (i = 0; i < m; i++) {
+    src[i] = (int32_t)g_below(g_draw(seed, 101, (uint64_t)i), (uint64_t)n);
+    dst[i] = (int32_t)g_below(g_draw(seed, 102, (uint64_t)i), (uint64_t)n);
+  }
+}
+
+/* Zipf(s) labels in [0, nlabels): label k with probability (k+1)^-s / H,
+ * from draw stream 301 by inverting the cumulative table. */
+void orc_gen_zipf_labels(int64_t n, int nlabels, double s, uint64_t seed, int32_t *labels, int threads) {
+  double *cdf = (double *)malloc(sizeof(double) * (size_t)(nlabels > 0 ? nlabels : 1));
+  double tot = 0, acc = 0;
+  int k;
+  int64_t i;
+  for (k = 0; k < nlabels; k++) tot += 1.0 / pow((double)(k + 1), s);
+  for (k = 0; k < nlabels; k++) {
+    acc += 1.0 / pow((double)(k + 1), s) / tot;
+    cdf[k] = acc;
+  }
+  cdf[nlabels - 1] = 1.0;
+  set_threads(threads);
+#pragma omp parallel for schedule(static)
+  for (i = 0; i < n; i++) {
+    const double r = g_unit(g_draw(seed, 301, (uint64_t)i));
+    int j = 0;
+    while (j < nlabels - 1 && r >= cdf[j]) j++;
+    labels[i] = j;
+  }
+  free(cdf);
+}
+
+/* Writes a symmetric CSR with labels in sub_ceci's "t n m / v id label degree
+ * / e u v" format (sub_ceci/graph/graph.cpp:86-166 reads it), each undirected
+ * edge once as u < v.  Returns the bytes written, -1 on an I/O error. */
+int64_t orc_write_tve(const char *path, int64_t n, const int64_t *off, const int32_t *idx,
+                      const int32_t *labels) {
+  FILE *f = fopen(path, "wb");
+  const size_t cap = (size_t)1 << 22;
+  char *buf, *p;
+  int64_t total = 0, u, e;
+  if (!f) return -1;
+  buf = (char *)malloc(cap + 96);
+  p = buf;
+#define TVE_FLUSH()                                                            \
+  if ((size_t)(p - buf) >= cap) {                                              \
+    if (fwrite(buf, 1, (size_t)(p - buf), f) != (size_t)(p - buf)) total = -1; \
+    if (total >= 0) total += p - buf;                                          \
+    p = buf;                                                                   \
+  }
+  *p++ = 't';
+  *p++ = ' ';
+  p = put_u64(p, (uint64_t)n);
+  *p++ = ' ';
+  p = put_u64(p, (uint64_t)(off[n] / 2));
+  *p++ = '\n';
+  for (u = 0; u < n; u++) {
+    *p++ = 'v';
+    *p++ = ' ';
+    p = put_u64(p, (uint64_t)u);
+    *p++ = ' ';
+    p = put_u64(p, (uint64_t)labels[u]);
+    *p++ = ' ';
+    p = put_u64(p, (uint64_t)(off[u + 1] - off[u]));
+    *p++ = '\n';
+    TVE_FLUSH()
+  }
+  for (u = 0; u < n; u++)
+    for (e = off[u]; e < off[u + 1]; e++) {
+      if (idx[e] <= u) continue;
+      *p++ = 'e';
+      *p++ = ' ';
+      p = put_u64(p, (uint64_t)u);
+      *p++ = ' ';
+      p = put_u64(p, (uint64_t)idx[e]);
+      *p++ = '\n';
+      TVE_FLUSH()
+    }
+#undef TVE_FLUSH
+  if (p > buf) {
+    if (fwrite(buf, 1, (size_t)(p - buf), f) != (size_t)(p - buf)) total = -1;
+    if (total >= 0) total += p - buf;
+  }
+  free(buf);
+  if (fclose(f) != 0) total = -1;
+  return total;
+}
+
+/* Chung-Lu with expected degrees w_i ~ (i + i0)^(-1/(gamma-1)): i0 is the
+ * offset at which vertex 0's expected degree equals the structural cut-off
+ * sqrt(n * mean_deg) (found by bisection), and each endpoint is drawn by
+ * inverting the continuous weight profile's CDF (draw streams 201 / 202);
+ * round(n * mean_deg / 2) draws.  Returns that edge count; src may be NULL to
+ * ask for it. */
+int64_t orc_gen_chung_lu(int64_t n, double gamma, double mean_deg, uint64_t seed, int32_t *src, int32_t *dst,
+                         int threads) {
+  const int64_t m = llround((double)n * mean_deg / 2.0);
+  const double alpha = 1.0 / (gamma - 1.0), a1 = 1.0 - alpha, target = sqrt((double)n * mean_deg);
+  double lo = 0.0, hi = (double)n, i0, base, span, inv;
+  int it;
+  int64_t i;
+  if (!src) return m;
+  for (it = 0; it < 100; it++) {
+    const double mid = 0.5 * (lo + hi);
+    const double integral = (pow((double)n + mid, a1) - pow(mid, a1)) / a1;
+    const double w0 = mean_deg * (double)n * pow(mid, -alpha) / integral;
+    if (w0 > target) lo = mid;
+    else hi = mid;
+  }
+  i0 = 0.5 * (lo + hi);
+  if (i0 < 1e-9) i0 = 1e-9;
+  base = pow(i0, a1);
+  span = pow((double)n + i0, a1) - base;
+  inv = 1.0 / a1;
+  set_threads(threads);
+#pragma omp parallel for schedule(static)
+  for (i = 0; i < m; i++) {
+    int e;
+    for (e = 0; e < 2; e++) {
+      const double q = base + g_unit(g_draw(seed, e ? 202 : 201, (uint64_t)i)) * span;
+      int64_t k = (int64_t)(pow(q, inv) - i0);
+      if (k < 0) k = 0;
+      if (k >= n) k = n - 1;
+      if (e) dst[i] = (int32_t)k;
+      else src[i] = (int32_t)k;
+    }
+  }
+  return m;
 }

@@ -43,12 +43,18 @@ uint64_t orc_tc_tasks(int64_t n, const int64_t *doff, const int32_t *didx, const
 /* k-clique count on the DAG, src/CFSolver.cuh:15-97 (k=4,5) generalised to
  * any k>=3 by the same nested materialised intersections. */
 uint64_t orc_clique(int64_t n, const int64_t *doff, const int32_t *didx, int k, int threads);
+/* orc_clique restricted to the first-vertex tasks u with keep[u] != 0. */
+uint64_t orc_clique_tasks(int64_t n, const int64_t *doff, const int32_t *didx, int k, const uint8_t *keep,
+                          int threads);
 
 /* Motif4_G2Miner restatement, src/gpu_kernels/G2Miner_kernels.cuh:438-552, on
  * the symmetric graph.  out[0..5] = 3-star, 4-path, tailed triangle, 4-cycle,
  * diamond, 4-clique. */
 void orc_motif4_g2miner(int64_t n, const int64_t *off, const int32_t *idx,
                         uint64_t *out, int threads);
+/* orc_motif4_g2miner restricted to the edge tasks of vertices with keep[v] != 0. */
+void orc_motif4_tasks(int64_t n, const int64_t *off, const int32_t *idx, const uint8_t *keep,
+                      uint64_t *out, int threads);
 
 /* P1..P8_G2Miner restatements, src/gpu_kernels/G2Miner_kernels.cuh:6-435. */
 uint64_t orc_pattern_g2miner(int64_t n, const int64_t *off, const int32_t *idx,
@@ -81,6 +87,23 @@ int64_t orc_write_mtx(const char *path, int64_t n, const int64_t *off, const int
 uint64_t orc_match(int64_t n, const int64_t *off, const int32_t *idx, const int32_t *labels,
                    int64_t qn, const int64_t *qoff, const int32_t *qidx,
                    const int32_t *qlabels, int threads);
+
+/* Seeded synthetic generators: the engine's own draws (splitmix64 finaliser
+ * over (seed, stream, index)) written again here, so that harnesses which
+ * must not load the engine build the same graphs.  R-MAT: m edges of
+ * 2^scale vertices, quadrant probabilities a, b, c; ER: m uniform draws;
+ * labels: Zipf(s) over [0, nlabels). */
+void orc_gen_rmat(int scale, int64_t m, double a, double b, double c, uint64_t seed, int32_t *src,
+                  int32_t *dst, int threads);
+void orc_gen_er(int64_t n, int64_t m, uint64_t seed, int32_t *src, int32_t *dst, int threads);
+int64_t orc_gen_chung_lu(int64_t n, double gamma, double mean_deg, uint64_t seed, int32_t *src, int32_t *dst,
+                         int threads);
+void orc_gen_zipf_labels(int64_t n, int nlabels, double s, uint64_t seed, int32_t *labels, int threads);
+
+/* A symmetric labelled CSR as sub_ceci's "t/v/e" text (each undirected edge
+ * once, u < v); bytes written or -1. */
+int64_t orc_write_tve(const char *path, int64_t n, const int64_t *off, const int32_t *idx,
+                      const int32_t *labels);
 
 #ifdef __cplusplus
 }

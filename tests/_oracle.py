@@ -22,12 +22,16 @@ def lib():
         if not os.path.exists(ORACLE_SO):
             raise ImportError(f"{ORACLE_SO} missing: run `make -C {os.path.dirname(ORACLE_SO)}`")
         L = ctypes.CDLL(ORACLE_SO)
-        for f in ("orc_tc", "orc_tc_tasks", "orc_tc_merge", "orc_clique", "orc_pattern_g2miner", "orc_pattern_solver", "orc_match"):
+        for f in ("orc_tc", "orc_tc_tasks", "orc_tc_merge", "orc_clique", "orc_clique_tasks", "orc_pattern_g2miner", "orc_pattern_solver", "orc_match"):
             getattr(L, f).restype = c_uint64
         L.orc_build_csr.restype = c_int64
         L.orc_orient.restype = c_int64
         L.orc_write_mtx.restype = c_int64
         L.orc_tc_weighted.restype = c_uint64
+        L.orc_write_tve.restype = c_int64
+        L.orc_gen_chung_lu.restype = c_int64
+        for f in ("orc_gen_rmat", "orc_gen_er", "orc_gen_zipf_labels"):
+            getattr(L, f).restype = None
         _lib = L
     return _lib
 
@@ -72,6 +76,18 @@ def tc_merge(doff, didx):
 
 def clique(doff, didx, k, threads=0):
     return lib().orc_clique(c_int64(len(doff) - 1), _p(doff), _p(didx), c_int(k), c_int(threads))
+
+
+def clique_tasks(doff, didx, k, keep, threads=0):
+    keep = np.ascontiguousarray(keep, np.uint8)
+    return lib().orc_clique_tasks(c_int64(len(doff) - 1), _p(doff), _p(didx), c_int(k), _p(keep), c_int(threads))
+
+
+def motif4_tasks(off, idx, keep, threads=0):
+    keep = np.ascontiguousarray(keep, np.uint8)
+    out = (c_uint64 * 6)()
+    lib().orc_motif4_tasks(c_int64(len(off) - 1), _p(off), _p(idx), _p(keep), out, c_int(threads))
+    return np.array(list(out), np.uint64)
 
 
 def motif4(off, idx, threads=0):
@@ -167,3 +183,49 @@ def two_hub_graph(n, m_rand, d0, d1, mids, seed):
         parts.append(np.stack([np.full(dh, h), nb], 1))
     e = np.concatenate(parts).astype(np.int32)
     return build_csr(n, e[:, 0], e[:, 1])
+
+
+def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, threads=0):
+    """The engine's seeded R-MAT draws, restated in the oracle (same edges as
+    gpm.gen_rmat without loading the engine)."""
+    m = (1 << scale) * edge_factor
+    src = np.empty(m, np.int32)
+    dst = np.empty(m, np.int32)
+    lib().orc_gen_rmat(c_int(scale), c_int64(m), ctypes.c_double(a), ctypes.c_double(b), ctypes.c_double(c),
+                       c_uint64(seed), _p(src), _p(dst), c_int(threads))
+    return 1 << scale, src, dst
+
+
+def gen_er(n, m, seed=1, threads=0):
+    src = np.empty(m, np.int32)
+    dst = np.empty(m, np.int32)
+    lib().orc_gen_er(c_int64(n), c_int64(m), c_uint64(seed), _p(src), _p(dst), c_int(threads))
+    return n, src, dst
+
+
+def gen_chung_lu(n, gamma, mean_deg, seed=1, threads=0):
+    m = lib().orc_gen_chung_lu(c_int64(n), ctypes.c_double(gamma), ctypes.c_double(mean_deg), c_uint64(seed), None,
+                               None, c_int(threads))
+    src = np.empty(m, np.int32)
+    dst = np.empty(m, np.int32)
+    lib().orc_gen_chung_lu(c_int64(n), ctypes.c_double(gamma), ctypes.c_double(mean_deg), c_uint64(seed), _p(src),
+                           _p(dst), c_int(threads))
+    return n, src, dst
+
+
+def gen_zipf_labels(n, nlabels, s=1.2, seed=1, threads=0):
+    lab = np.empty(n, np.int32)
+    lib().orc_gen_zipf_labels(c_int64(n), c_int(nlabels), ctypes.c_double(s), c_uint64(seed), _p(lab),
+                              c_int(threads))
+    return lab
+
+
+def write_tve(path, off, idx, labels):
+    """Symmetric labelled CSR as sub_ceci's t/v/e text."""
+    off = np.ascontiguousarray(off, np.int64)
+    idx = np.ascontiguousarray(idx, np.int32)
+    labels = np.ascontiguousarray(labels, np.int32)
+    r = lib().orc_write_tve(str(path).encode(), c_int64(len(off) - 1), _p(off), _p(idx), _p(labels))
+    if r < 0:
+        raise OSError(f"writing {path} failed")
+    return r

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures in tests/golden from the AntiRF reference.
 
-Run in a container where the reference is mounted (default /root/reference)
-and oracle/_ref/myceci has been built (`make -C oracle`):
+Run in a container where the reference is mounted (REFERENCE_DIR, else
+$GPM_REF_DIR, else oracle/Makefile's REF_DIR) and oracle/_ref/myceci has been
+built (`make -C oracle`):
 
     python tests/golden/make_golden.py [REFERENCE_DIR]
 
@@ -81,7 +82,17 @@ SHAPES = {
 }
 
 
-def main(ref="/root/reference"):
+def default_ref_dir():
+    if os.environ.get("GPM_REF_DIR"):
+        return os.environ["GPM_REF_DIR"]
+    for line in open(os.path.join(ROOT, "oracle", "Makefile")):
+        if line.startswith("REF_DIR") and "?=" in line:
+            return line.split("?=", 1)[1].strip()
+    raise SystemExit("give the reference's directory (argument or GPM_REF_DIR)")
+
+
+def main(ref=None):
+    ref = ref or default_ref_dir()
     ceci = os.path.join(ref, "sub_ceci", "test")
     # ---- HPRD KATs
     n, e, lab = read_tve(os.path.join(ceci, "data_graph", "HPRD.graph"))

@@ -63,3 +63,19 @@ def test_over_ranks_single():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.over_ranks(None, None, 3.5, 42) == (3.5, 42.0)
+
+
+def test_reference_arm_never_loads_the_engine():
+    # the reference arm times the reference's CPU implementation (the oracle
+    # port, sub_ceci); its process must not map libgpm.so at all
+    import subprocess
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'tc', '--scale', '12', "
+            "'--steps', '1', '--warmup', '1', '--cpu-seconds', '0.2', '--no-ref-gpu']; sys.path.insert(0, '.'); "
+            "import bench; bench.main(); "
+            "print('MAPS', sum('libgpm' in l for l in open('/proc/self/maps')))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = out.stdout.strip().splitlines()
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["one_core"]["cores"] == 1
+    assert lines[-1] == "MAPS 0"

@@ -102,3 +102,35 @@ def test_device_calls_fail_cleanly_without_gpu():
     with pytest.raises(gpm.GpmError) as e:
         gpm.Graph.from_edges(3, [0, 1], [1, 2])
     assert e.value.status == 7
+
+
+def test_oracle_generators_match_the_engine():
+    # bench.py's reference arm and the fixture scripts build their graphs with
+    # the oracle's restated generators so that they never load the engine;
+    # the edges must be the engine's own, draw for draw
+    for scale, ef, seed in ((10, 16, 7), (15, 4, 1)):
+        a, b = orc.gen_rmat(scale, ef, seed=seed), gpm.gen_rmat(scale, ef, seed=seed)
+        assert a[0] == b[0] and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    a, b = orc.gen_rmat(12, 8, 0.45, 0.15, 0.15, seed=3), gpm.gen_rmat(12, 8, 0.45, 0.15, 0.15, seed=3)
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    a, b = orc.gen_er(5000, 40000, seed=3), gpm.gen_er(5000, 40000, seed=3)
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    import workloads
+    n, gam, md = workloads.batch_members()
+    for m in (0, 111, 222):
+        a = orc.gen_chung_lu(int(n[m]), gam[m], md[m], seed=workloads.member_seed(m))
+        b = gpm.gen_chung_lu(int(n[m]), gam[m], md[m], seed=workloads.member_seed(m))
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+    for s in (1.2, 0.7):
+        assert np.array_equal(orc.gen_zipf_labels(100000, 8, s, seed=3), gpm.gen_zipf_labels(100000, 8, s, seed=3))
+
+
+def test_oracle_tve_writer(tmp_path):
+    n, s, d = orc.gen_rmat(8, 4, seed=2)
+    off, idx = orc.build_csr(n, s, d)
+    lab = orc.gen_zipf_labels(n, 3, 1.2, seed=2)
+    path = tmp_path / "g.graph"
+    orc.write_tve(path, off, idx, lab)
+    n2, s2, d2, lab2 = gpm.read_tve(str(path))
+    off2, idx2 = orc.build_csr(n2, s2, d2)
+    assert n2 == n and np.array_equal(off2, off) and np.array_equal(idx2, idx) and np.array_equal(lab2, lab)

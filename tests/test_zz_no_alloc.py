@@ -41,11 +41,16 @@ def test_noalloc_matches_allocating_entry_point(scale, relabel):
     torch.cuda.synchronize()
     want = int(ref.item())
     assert want == g.tc(gpm.V_CENTRIC) > 0
-    for _ in range(2):
-        out = torch.full((1,), -1, dtype=torch.int64, device=dev)
+    outs = [torch.full((1,), -1, dtype=torch.int64, device=dev) for _ in range(3)]
+    gpm.check(_call(len(off) - 1, off_t, idx_t, outs[0], stream))  # first call: per-device set-up
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(dev)[0]
+    for out in outs[1:]:
         gpm.check(_call(len(off) - 1, off_t, idx_t, out, stream))
         torch.cuda.synchronize()
-        assert int(out.item()) == want
+    # device memory in use is unchanged by the later calls: they allocated nothing
+    assert torch.cuda.mem_get_info(dev)[0] == free_before
+    assert [int(o.item()) for o in outs] == [want] * 3
 
 
 def test_noalloc_rejects_oversized_graph():
