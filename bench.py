@@ -304,13 +304,19 @@ def cpu_match_ceci(off, idx, labels, queries, num):
                 f.write(f"t {k} {len(e)}\n")
                 f.writelines(f"v {v} {int(ql[v])} {deg[v]}\n" for v in range(k))
                 f.writelines(f"e {int(a)} {int(b)}\n" for a, b in e)
-            procs[name] = subprocess.Popen([exe, "-d", data, "-q", qp, "-filter", "CECI", "-order", "CECI",
-                                            "-engine", "CECI", "-num", str(int(num))],
-                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        for name, p in procs.items():
+            # sub_ceci prints two lines per search call (hundreds of MB here):
+            # only the summary at the end is kept
+            p1 = subprocess.Popen([exe, "-d", data, "-q", qp, "-filter", "CECI", "-order", "CECI", "-engine", "CECI",
+                                   "-num", str(int(num))], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL)
+            procs[name] = (p1, subprocess.Popen(["tail", "-n", "40"], stdin=p1.stdout, stdout=subprocess.PIPE,
+                                                text=True))
+            p1.stdout.close()
+        for name, (p1, p) in procs.items():
             try:
                 out, _ = p.communicate(timeout=900)
+                p1.wait(timeout=60)
             except subprocess.TimeoutExpired:
+                p1.kill()
                 p.kill()
                 res[name] = {"unavailable": "no result within 900 s"}
                 continue

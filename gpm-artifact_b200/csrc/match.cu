@@ -8,14 +8,13 @@
 //
 // GPU design: the query (<= 16 vertices) is ordered on the host -- start at
 // the vertex whose label is rarest in the data graph (ties: higher degree),
-// then repeatedly the unplaced vertex with most placed neighbours.  Each
-// later vertex has a parent (its first placed neighbour, whose data
-// neighbours are the candidates) and back-neighbours (checked by binary
-// search in their images' sorted lists).  One warp per root candidate runs
-// the depth-first extension: a level's candidates are filtered by label,
-// degree, injectivity and back-edges 32 at a time and compacted with ballots
-// into per-warp scratch; the last level is only counted.  Work is drained
-// from an atomic root cursor.
+// then repeatedly the unplaced vertex with most placed neighbours.  The data
+// graph's lists are partitioned by label, so the candidates of a query
+// vertex are one label segment of a mapped neighbour's list (the shortest
+// one), and the other back-edges are checked by one bit test (vertices with
+// an adjacency bitmap) or a binary search inside a label segment.  Tasks are
+// the (root, second vertex) pairs, drained from an atomic cursor by a
+// persistent grid; each warp walks its task depth first (k_match).
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -92,28 +91,175 @@ __device__ __forceinline__ bool has_edge_label(const int64_t *__restrict__ off, 
   return false;
 }
 
-// n = number of (root, second vertex) pairs.  TRACK: every embedding found
-// takes a slot of *found; those below `limit` are written to emb_out (when
-// given: q.n data-vertex ids per embedding, in query-vertex order), and the
-// whole grid stops once `limit` are found (sub_ceci's -num,
-// myceci.cpp:615-617).  Otherwise the count goes to *out.
+// Adjacency bitmaps of the high-degree vertices (cached with the label
+// partition): hub slot of v (or -1) and, per hub, one bit per vertex id.  A
+// membership test against a hub is one load instead of a binary search of up
+// to log2(degree) dependent loads; the index trades HBM capacity (a few GB on
+// R-MAT 21) for probe latency.
+struct HubIndex {
+  const int32_t *slot;  // n: bitmap row of v, -1 when v has no bitmap
+  const uint32_t *bm;   // rows x words
+  int64_t words;        // (n + 31) / 32
+};
+
+// Is x a neighbour of a with label l?  Bit test when a has a bitmap, else a
+// binary search in a's label segment (x carries label l).
+__device__ __forceinline__ bool adjacent(const HubIndex &hub, const int64_t *__restrict__ off,
+                                         const int32_t *__restrict__ adj, const int32_t *__restrict__ ladj,
+                                         const int32_t *__restrict__ loff, int L, int32_t a, int l, int32_t x) {
+  const int32_t hs = hub.slot[a];
+  if (hs >= 0) return (__ldg(hub.bm + hs * hub.words + (x >> 5)) >> (x & 31)) & 1u;
+  return has_edge_label(off, adj, ladj, loff, L, a, l, x);
+}
+
+// Warp-level depth-first enumeration over (root, second vertex) tasks.
+// Positions 2 .. n-2 walk their candidates lazily: the candidate source of a
+// position is the shortest label segment among its mapped query-neighbours;
+// 32 entries at a time are filtered (label, degree bound, injectivity, the
+// other back-edges) and the survivors compacted into the warp's shared
+// buffer of that position, so no candidate list is materialised in global
+// memory and every SM keeps its full warp complement.  The last position is
+// counted without a stack level: for all survivors y of one chunk of
+// position n-2 at once, the last vertex's candidate segments (each y's
+// shortest) are laid end to end and every lane takes one entry of the
+// concatenation, so short segments do not leave lanes idle.
+// TRACK: every embedding found takes a slot of *found; those below `limit`
+// are written to emb_out (when given: q.n data-vertex ids per embedding, in
+// query-vertex order), and the whole grid stops once `limit` are found
+// (sub_ceci's -num, myceci.cpp:615-617).  Otherwise the count goes to *out.
+constexpr int kMatchWarps = 8;
 template <bool TRACK>
-__global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restrict__ pairs, int64_t n,
-                                               const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
-                                               const int32_t *__restrict__ ladj, const int32_t *__restrict__ loff,
-                                               int L, const int32_t *__restrict__ labels,
-                                               int32_t *__restrict__ scratch, int64_t maxd,
-                                               unsigned long long *__restrict__ cursor,
-                                               unsigned long long *__restrict__ out, unsigned long long limit,
-                                               unsigned long long *found, int32_t *__restrict__ emb_out) {
+__global__ void __launch_bounds__(kMatchWarps * 32)
+    k_match(QueryPlan q, const int2 *__restrict__ pairs, int64_t n, const int64_t *__restrict__ off,
+            const int32_t *__restrict__ adj, const int32_t *__restrict__ ladj, const int32_t *__restrict__ loff,
+            int L, const int32_t *__restrict__ labels, HubIndex hub, unsigned long long *__restrict__ cursor,
+            unsigned long long *__restrict__ out, unsigned long long limit, unsigned long long *found,
+            int32_t *__restrict__ emb_out) {
+  __shared__ int32_t sbuf[kMatchWarps][kMaxQ - 2][32];
   const unsigned lane = lane_id();
-  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  int32_t *lists = scratch + warp * maxd * (kMaxQ - 1);
-  int32_t emb[kMaxQ];
-  int cur[kMaxQ], sz[kMaxQ];
+  int32_t(*buf)[32] = sbuf[threadIdx.x >> 5];
+  int32_t emb[kMaxQ] = {};
+  int64_t pos[kMaxQ], end[kMaxQ];
+  uint32_t chk[kMaxQ];
+  int bcnt[kMaxQ], bcur[kMaxQ];
+  const int last = q.n - 1, pre = q.n - 2;
+  const int llab = q.label[last];
+  const uint32_t lmask = q.back_pos[last] | (1u << q.parent_pos[last]);
   unsigned long long c = 0;
-  // tasks are the (root, second vertex) pairs: parallelism over edges, not
-  // roots, so a hub root's subtree is spread over many warps
+
+  // candidate segment of position d: the shortest label segment among the
+  // mapped query-neighbours, the others left to check (chk)
+  auto open = [&](int d) {
+    const int lab = q.label[d];
+    uint32_t nb = q.back_pos[d] | (1u << q.parent_pos[d]);
+    int src = q.parent_pos[d];
+    int64_t s, e;
+    seg_range(off, loff, L, emb[src], lab, &s, &e);
+    if (L > 0)
+      for (uint32_t bm = q.back_pos[d]; bm; bm &= bm - 1) {
+        const int j = __ffs(bm) - 1;
+        int64_t sj, ej;
+        seg_range(off, loff, L, emb[j], lab, &sj, &ej);
+        if (ej - sj < e - s) {
+          src = j;
+          s = sj;
+          e = ej;
+        }
+      }
+    chk[d] = nb & ~(1u << src);
+    pos[d] = off[emb[src]] + s;
+    end[d] = off[emb[src]] + e;
+  };
+
+  // next chunk of position d's candidates into buf[d - 2]; returns survivors
+  auto fill = [&](int d) -> int {
+    const int lab = q.label[d];
+    const int64_t i = pos[d] + lane;
+    bool ok = false;
+    int32_t x = 0;
+    if (i < end[d]) {
+      x = __ldg(ladj + i);
+      ok = (L > 0 || labels[x] == lab) && off[x + 1] - off[x] >= q.mindeg[d];
+      for (int j = 0; ok && j < d; ++j) ok = emb[j] != x;
+      for (uint32_t bm = chk[d]; ok && bm; bm &= bm - 1)
+        ok = adjacent(hub, off, adj, ladj, loff, L, emb[__ffs(bm) - 1], lab, x);
+    }
+    pos[d] += 32;
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (ok) buf[d - 2][__popc(m & ((1u << lane) - 1u))] = x;
+    __syncwarp();
+    return __popc(m);
+  };
+
+  // embeddings completing positions 0 .. n-3 with y = ys (lane t < k holds
+  // candidate t of position n-2) and some last vertex
+  auto close = [&](int32_t y, int k) {
+    // lane t: its candidate's shortest segment for the last vertex
+    int src = -1;
+    long long st = 0, len = 0;
+    if ((int)lane < k) {
+      for (uint32_t bm = lmask; bm; bm &= bm - 1) {
+        const int j = __ffs(bm) - 1;
+        const int32_t a = j == pre ? y : emb[j];
+        int64_t s, e;
+        seg_range(off, loff, L, a, llab, &s, &e);
+        if (src < 0 || e - s < len) {
+          src = j;
+          st = off[a] + s;
+          len = e - s;
+        }
+      }
+    }
+    long long inc = len;  // inclusive prefix over the lanes
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long v = __shfl_up_sync(0xffffffffu, inc, o);
+      if ((int)lane >= o) inc += v;
+    }
+    const long long total = __shfl_sync(0xffffffffu, inc, 31);
+    for (long long base = 0; base < total; base += 32) {
+      const long long idx = base + lane;
+      // t = first lane whose inclusive prefix exceeds idx
+      int lo = 0, hi = 31;
+#pragma unroll
+      for (int r = 0; r < 5; ++r) {
+        const int mid = (lo + hi) >> 1;
+        const long long pm = __shfl_sync(0xffffffffu, inc, mid);
+        if (pm > idx) hi = mid; else lo = mid + 1;
+      }
+      const int t = lo;
+      const long long pt = __shfl_sync(0xffffffffu, inc, t), lt = __shfl_sync(0xffffffffu, len, t);
+      const long long stt = __shfl_sync(0xffffffffu, st, t);
+      const int srct = __shfl_sync(0xffffffffu, src, t);
+      const int32_t yt = __shfl_sync(0xffffffffu, y, t);
+      bool ok = false;
+      int32_t x = 0;
+      if (idx < total) {
+        x = __ldg(ladj + stt + (idx - (pt - lt)));
+        ok = (L > 0 || labels[x] == llab) && x != yt;
+        for (int j = 0; ok && j < pre; ++j) ok = emb[j] != x;
+        for (uint32_t bm = lmask & ~(1u << srct); ok && bm; bm &= bm - 1) {
+          const int j = __ffs(bm) - 1;
+          ok = adjacent(hub, off, adj, ladj, loff, L, j == pre ? yt : emb[j], llab, x);
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (TRACK && m) {
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(found, (unsigned long long)__popc(m));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        const unsigned long long slot = at + __popc(m & ((1u << lane) - 1u));
+        if (emb_out && ok && slot < limit) {
+          int32_t *row = emb_out + slot * (unsigned long long)q.n;
+          for (int j = 0; j < pre; ++j) row[q.order[j]] = emb[j];
+          row[q.order[pre]] = yt;
+          row[q.order[last]] = x;
+        }
+      }
+      c += lane == 0 ? (unsigned long long)__popc(m) : 0ull;
+    }
+  };
+
   while (true) {
     unsigned long long r = 0;
     if (lane == 0) r = atomicAdd(cursor, 1ull);
@@ -123,88 +269,37 @@ __global__ void __launch_bounds__(256) k_match(QueryPlan q, const int2 *__restri
     const int2 pr = pairs[r];
     emb[0] = pr.x;
     emb[1] = pr.y;
-    int depth = 2;  // position being filled
-    bool build = true;
-    while (depth >= 2) {
-      if (build) {
-        // candidates of position `depth`: the neighbours with the position's
-        // label of whichever mapped query-neighbour has the fewest (one
-        // segment of the label-partitioned list); the other mapped
-        // query-neighbours are checked inside their own segments
-        const int lab = q.label[depth];
-        uint32_t nb = q.back_pos[depth] | (1u << q.parent_pos[depth]);
-        int src = q.parent_pos[depth];
-        int64_t s, e;
-        seg_range(off, loff, L, emb[src], lab, &s, &e);
-        if (L > 0 && q.back_pos[depth]) {
-          for (uint32_t bm = q.back_pos[depth]; bm; bm &= bm - 1) {
-            const int j = __ffs(bm) - 1;
-            int64_t sj, ej;
-            seg_range(off, loff, L, emb[j], lab, &sj, &ej);
-            if (ej - sj < e - s) {
-              src = j;
-              s = sj;
-              e = ej;
-            }
-          }
-        }
-        nb &= ~(1u << src);
-        const int32_t *seg = ladj + off[emb[src]];
-        const bool last = depth == q.n - 1;
-        int32_t *Lst = lists + (int64_t)(depth - 2) * maxd;
-        int cnt = 0;
-        for (int64_t base = s; base < e; base += 32) {
-          int64_t i = base + lane;
-          bool ok = false;
-          int32_t x = 0;
-          if (i < e) {
-            x = __ldg(seg + i);
-            // a label segment holds only that label (L > 0); at the last
-            // level every query edge of the vertex is a back-edge checked
-            // below, so the degree bound prunes nothing there
-            ok = (L > 0 || labels[x] == lab) && (last || off[x + 1] - off[x] >= q.mindeg[depth]);
-            for (int j = 0; ok && j < depth; ++j) ok = emb[j] != x;
-            uint32_t bm = nb;
-            while (ok && bm) {
-              int j = __ffs(bm) - 1;
-              bm &= bm - 1;
-              ok = has_edge_label(off, adj, ladj, loff, L, emb[j], lab, x);
-            }
-          }
-          unsigned m = __ballot_sync(0xffffffffu, ok);
-          if (!last && ok) Lst[cnt + __popc(m & ((1u << lane) - 1u))] = x;
-          if (TRACK && last && m) {
-            unsigned long long at = 0;
-            if (lane == 0) at = atomicAdd(found, (unsigned long long)__popc(m));
-            at = __shfl_sync(0xffffffffu, at, 0);
-            const unsigned long long slot = at + __popc(m & ((1u << lane) - 1u));
-            if (emb_out && ok && slot < limit) {
-              int32_t *row = emb_out + slot * (unsigned long long)q.n;
-              for (int j = 0; j < depth; ++j) row[q.order[j]] = emb[j];
-              row[q.order[depth]] = x;
-            }
-          }
-          cnt += __popc(m);
-        }
-        __syncwarp();
-        if (last) {
-          c += lane == 0 ? (unsigned long long)cnt : 0ull;
-          --depth;
-          build = false;
-          if (TRACK && *(volatile unsigned long long *)found >= limit) break;
+    if (pre == 1) {  // three query vertices: the pair's second vertex is position n-2
+      close(pr.y, 1);
+      continue;
+    }
+    int d = 2;
+    open(2);
+    bcnt[2] = bcur[2] = 0;
+    while (d >= 2) {
+      if (TRACK && *(volatile unsigned long long *)found >= limit) break;
+      if (d == pre) {
+        if (pos[d] >= end[d]) {
+          --d;
           continue;
         }
-        sz[depth] = cnt;
-        cur[depth] = 0;
-        build = false;
-      }
-      if (cur[depth] >= sz[depth]) {
-        --depth;
+        const int k = fill(d);
+        if (k) close((int)lane < k ? buf[d - 2][lane] : 0, k);
         continue;
       }
-      emb[depth] = lists[(int64_t)(depth - 2) * maxd + cur[depth]++];
-      ++depth;
-      build = true;
+      if (bcur[d] < bcnt[d]) {
+        emb[d] = buf[d - 2][bcur[d]++];
+        ++d;
+        open(d);
+        bcnt[d] = bcur[d] = 0;
+        continue;
+      }
+      if (pos[d] < end[d]) {
+        bcnt[d] = fill(d);
+        bcur[d] = 0;
+        continue;
+      }
+      --d;
     }
   }
   if (TRACK) return;
@@ -344,6 +439,11 @@ static int plan_query(const gpm_query *q, const std::vector<int64_t> &label_freq
 struct LabelCsr {
   int L = 0;  // partitions (max label + 1); 0: labels too wide, lists copied as they are
   DevBuf<int32_t> ladj, loff;
+  // adjacency bitmaps of the vertices with at least hub_min neighbours
+  DevBuf<int32_t> hub_slot;
+  DevBuf<uint32_t> hub_bm;
+  int64_t hub_words = 0;
+  int hubs = 0, hub_min = 0;
 };
 void free_label_csr(LabelCsr *p) { delete p; }
 
@@ -352,6 +452,87 @@ __global__ void k_label_range(int64_t n, const int32_t *__restrict__ labels, int
     atomicMax(&mm[0], labels[i]);
     atomicMin(&mm[1], labels[i]);
   }
+}
+
+__global__ void k_deg_hist(int64_t n, const int64_t *__restrict__ off, unsigned long long *__restrict__ h) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t d = off[v + 1] - off[v];
+    atomicAdd(&h[d > 0 ? 64 - __clzll((unsigned long long)d) : 0], 1ull);  // bin b: 2^(b-1) <= d < 2^b
+  }
+}
+__global__ void k_hub_slots(int64_t n, const int64_t *__restrict__ off, int64_t dmin, int32_t *__restrict__ slot,
+                            int *__restrict__ cnt) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    slot[v] = off[v + 1] - off[v] >= dmin ? atomicAdd(cnt, 1) : -1;
+}
+__global__ void k_hub_fill(int64_t n, const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                           const int32_t *__restrict__ slot, int64_t words, uint32_t *__restrict__ bm) {
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = warp; v < n; v += nw) {
+    const int32_t hs = slot[v];
+    if (hs < 0) continue;
+    uint32_t *row = bm + hs * words;
+    for (int64_t k = off[v] + lane_id(); k < off[v + 1]; k += 32) {
+      const int32_t x = adj[k];
+      atomicOr(row + (x >> 5), 1u << (x & 31));
+    }
+  }
+}
+
+// Adjacency bitmaps for the highest-degree vertices: the smallest power-of-two
+// degree bound (at least kHubMinDegree) whose bitmaps fit the byte budget
+// (GPM_HUB_BITMAP_BYTES, default 8 GiB, at most a quarter of the free memory).
+constexpr int64_t kHubMinDegree = 256;
+static int build_hub_index(gpm_graph *g, LabelCsr *lc) {
+  const int64_t n = g->n, words = (n + 31) / 32;
+  GPM_TRY(lc->hub_slot.reserve(std::max<int64_t>(n, 1)));
+  lc->hub_words = words;
+  if (n == 0) return GPM_OK;
+  DevBuf<unsigned long long> h;
+  GPM_TRY(h.reserve(65));
+  GPM_CUDA(cudaMemset(h.p, 0, 65 * sizeof(unsigned long long)));
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 16);
+  k_deg_hist<<<blocks, 256>>>(n, g->off.p, h.p);
+  unsigned long long hist[65];
+  GPM_CUDA(cudaMemcpy(hist, h.p, sizeof hist, cudaMemcpyDeviceToHost));
+  size_t free_b = 0, total_b = 0;
+  GPM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  int64_t budget = (int64_t)8 << 30;
+  if (const char *e = getenv("GPM_HUB_BITMAP_BYTES")) budget = atoll(e);
+  budget = std::min<int64_t>(budget, (int64_t)(free_b / 4));
+  // vertices with degree >= 2^(b-1) are those in bins b .. 64
+  int64_t dmin = 0, count = 0;
+  for (int b = 1; b <= 64; ++b) {
+    unsigned long long above = 0;
+    for (int k = b; k <= 64; ++k) above += hist[k];
+    const int64_t d = (int64_t)1 << (b - 1);
+    if (d < kHubMinDegree) continue;
+    if ((int64_t)above * words * 4 <= budget) {
+      dmin = d;
+      count = (int64_t)above;
+      break;
+    }
+  }
+  DevBuf<int> cnt;
+  GPM_TRY(cnt.reserve(1));
+  GPM_CUDA(cudaMemset(cnt.p, 0, sizeof(int)));
+  if (count == 0) {
+    GPM_CUDA(cudaMemset(lc->hub_slot.p, 0xff, sizeof(int32_t) * n));
+    lc->hubs = 0;
+    lc->hub_min = 0;
+    GPM_TRY(lc->hub_bm.reserve(1));
+    return GPM_OK;
+  }
+  GPM_TRY(lc->hub_bm.reserve((size_t)(count * words)));
+  GPM_CUDA(cudaMemset(lc->hub_bm.p, 0, sizeof(uint32_t) * count * words));
+  k_hub_slots<<<blocks, 256>>>(n, g->off.p, dmin, lc->hub_slot.p, cnt.p);
+  k_hub_fill<<<(int)std::min<int64_t>((n * 32 + 255) / 256, (int64_t)num_sms() * 16), 256>>>(
+      n, g->off.p, g->adj.p, lc->hub_slot.p, words, lc->hub_bm.p);
+  GPM_LAUNCH_CHECK();
+  lc->hubs = (int)count;
+  lc->hub_min = (int)dmin;
+  return GPM_OK;
 }
 
 static int ensure_label_csr(gpm_graph *g) {
@@ -391,6 +572,7 @@ static int ensure_label_csr(gpm_graph *g) {
     k_label_offsets<<<(int)std::min<int64_t>((n * 32 + 255) / 256, num_sms() * 16), 256>>>(n, g->off.p, sorted.p, L,
                                                                                           lc->ladj.p, lc->loff.p);
   }
+  if ((s = build_hub_index(g, lc))) return bail(s);
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("label partition: ") + cudaGetErrorString(e)));
   g->lcsr = lc;
@@ -493,7 +675,6 @@ static int match_run(gpm_graph *g, const gpm_query *q, unsigned long long limit,
   }
   GPM_TRY(ensure_label_csr(g));
   LabelCsr *lc = g->lcsr;
-  const int64_t maxd = std::max(1, g->max_deg);
   const int blocks = (int)std::min<int64_t>((g->n * 32 + 255) / 256, (int64_t)num_sms() * 16);
   DevBuf<unsigned long long> d, npairs;
   GPM_TRY(d.reserve(1));
@@ -517,23 +698,25 @@ static int match_run(gpm_graph *g, const gpm_query *q, unsigned long long limit,
     GPM_LAUNCH_CHECK();
     return finish(np);
   }
-  int64_t warps = (int64_t)num_sms() * 4 * 8;
-  const int64_t cap_words = (int64_t)2 << 30;
-  while (warps > 32 && warps * maxd * (kMaxQ - 1) > cap_words) warps >>= 1;
-  DevBuf<int32_t> scratch;
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match<false>, kMatchWarps * 32, 0);
+    per_sm = std::max(1, per_sm);
+  }
+  const int grid = per_sm * num_sms();
+  const HubIndex hub{lc->hub_slot.p, lc->hub_bm.p, lc->hub_words};
   DevBuf<unsigned long long> cursor;
-  GPM_TRY(scratch.reserve((size_t)(warps * maxd * (kMaxQ - 1))));
   GPM_TRY(cursor.reserve(1));
   GPM_CUDA(cudaMemset(cursor.p, 0, 8));
   GPM_CUDA(cudaMemset(d.p, 0, 8));
   if (track)
-    k_match<true><<<(int)(warps / 8), 256>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p, lc->loff.p,
-                                             lc->L, g->labels.p, scratch.p, maxd, cursor.p, d.p, limit, found.p,
-                                             emb ? demb.p : nullptr);
+    k_match<true><<<grid, kMatchWarps * 32>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p, lc->loff.p,
+                                              lc->L, g->labels.p, hub, cursor.p, d.p, limit, found.p,
+                                              emb ? demb.p : nullptr);
   else
-    k_match<false><<<(int)(warps / 8), 256>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p,
-                                              lc->loff.p, lc->L, g->labels.p, scratch.p, maxd, cursor.p, d.p, limit,
-                                              found.p, nullptr);
+    k_match<false><<<grid, kMatchWarps * 32>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p,
+                                               lc->loff.p, lc->L, g->labels.p, hub, cursor.p, d.p, limit, found.p,
+                                               nullptr);
   GPM_LAUNCH_CHECK();
   unsigned long long h = 0;
   GPM_CUDA(cudaMemcpy(&h, track ? found.p : d.p, 8, cudaMemcpyDeviceToHost));

@@ -542,6 +542,55 @@ int gpm_sched_set_default(gpm_sched *s) {
   return GPM_OK;
 }
 
+// Logged cost (active warp-cycles) of every owner under each configuration:
+// cost[6 * v + c], 0 for vertices that own no task.
+int gpm_tc_task_costs(gpm_graph *g, float *cost) {
+  if (!g || !cost) return fail(GPM_EINVAL, "NULL argument");
+  cudaStream_t st = 0;
+  DevBuf<int32_t> tasks;
+  int nt = 0;
+  GPM_TRY(all_tasks(g, tasks, &nt, st));
+  DevBuf<unsigned long long> rec, cnt;
+  DevBuf<uint8_t> cfg;
+  GPM_TRY(rec.reserve(g->n));
+  GPM_TRY(cnt.reserve(1));
+  GPM_TRY(cfg.reserve(g->n));
+  std::vector<unsigned long long> h(g->n);
+  for (int c = 0; c < kOut; ++c) {
+    GPM_CUDA(cudaMemsetAsync(cfg.p, c, g->n, st));
+    RankPlan *p = nullptr;
+    GPM_TRY(rank_plan_new(g, kRankCtaMin, kRankLongMin, cfg.p, st, &p));
+    int s1 = rank_plan_launch(g, p, st, cnt.p, nullptr);  // warm the caches
+    if (s1 == GPM_OK && cudaMemsetAsync(rec.p, 0, sizeof(unsigned long long) * g->n, st) != cudaSuccess)
+      s1 = fail(GPM_ECUDA, "memset");
+    if (s1 == GPM_OK) s1 = rank_plan_launch(g, p, st, cnt.p, rec.p);
+    if (s1 == GPM_OK && cudaMemcpy(h.data(), rec.p, sizeof(unsigned long long) * g->n, cudaMemcpyDeviceToHost) !=
+                            cudaSuccess)
+      s1 = fail(GPM_ECUDA, "cost copy");
+    free_rank_plan(p);
+    if (s1 != GPM_OK) return s1;
+    for (int64_t v = 0; v < g->n; ++v) cost[6 * v + c] = (float)h[v];
+  }
+  return GPM_OK;
+}
+
+// An explicit per-owner configuration for GPM_TC_LEARNED on g (host cfg[v] in
+// 0..5): replaces whatever schedule the scheduler chose, until the graph's
+// plans are dropped or a scheduler is attached.
+int gpm_tc_set_schedule(gpm_graph *g, const uint8_t *cfg) {
+  if (!g || !cfg) return fail(GPM_EINVAL, "NULL argument");
+  for (int64_t v = 0; v < g->n; ++v)
+    if (cfg[v] >= kOut) return fail(GPM_EINVAL, "configuration out of range (0..5)");
+  DevBuf<uint8_t> d;
+  GPM_TRY(d.reserve(std::max<int64_t>(g->n, 1)));
+  if (g->n) GPM_CUDA(cudaMemcpy(d.p, cfg, g->n, cudaMemcpyHostToDevice));
+  RankPlan *p = nullptr;
+  GPM_TRY(rank_plan_new(g, kRankCtaMin, kRankLongMin, d.p, 0, &p));
+  free_rank_plan(g->learned);
+  g->learned = p;
+  return GPM_OK;
+}
+
 // Configuration each owner task would get: cfg[v] in 0..5 (255: no task).
 int gpm_sched_assign(gpm_sched *s, gpm_graph *g, uint8_t *cfg) {
   if (!s || !g || !cfg) return fail(GPM_EINVAL, "NULL argument");

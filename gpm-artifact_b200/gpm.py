@@ -87,6 +87,8 @@ _SIGS = {
     "gpm_sched_attach": ([_P, _P], c_int),
     "gpm_sched_set_default": ([_P], c_int),
     "gpm_sched_assign": ([_P, _P, _P], c_int),
+    "gpm_tc_task_costs": ([_P, _P], c_int),
+    "gpm_tc_set_schedule": ([_P, _P], c_int),
     "gpm_batch_create": ([c_int, _P, _P, _P, _P, POINTER(c_void_p)], c_int),
     "gpm_batch_generate_chung_lu": ([c_int, _P, _P, _P, c_uint64, POINTER(c_void_p)], c_int),
     "gpm_batch_info": ([_P, POINTER(c_int), POINTER(c_int64), POINTER(c_int64)], c_int),
@@ -308,6 +310,19 @@ class Graph:
         st = np.zeros(4, np.uint64)
         check(lib.gpm_tc_plan_stats(self.h, _ptr(st)))
         return tuple(int(x) for x in st)
+
+    def task_costs(self):
+        """Logged active warp-cycles of every owner task under each of the 6
+        scheduler configurations: float32[n, 6] (0 where v owns no task)."""
+        c = np.zeros((self.info().n, 6), np.float32)
+        check(lib.gpm_tc_task_costs(self.h, _ptr(c)))
+        return c
+
+    def set_schedule(self, cfg):
+        """Explicit per-owner configuration (uint8[n], 0..5) for TC_LEARNED."""
+        cfg = np.ascontiguousarray(cfg, np.uint8)
+        check(lib.gpm_tc_set_schedule(self.h, _ptr(cfg)))
+        return self
 
     def tc(self, mode=V_CENTRIC) -> int:
         out = c_uint64()

@@ -71,6 +71,70 @@ def run_er():
             "ms_per_count": res, "teps_bitmap": m / (res["bitmap"] / 1e3)}
 
 
+def count_ms(g, variant, reps=5, burst=5):
+    """Median over `reps` of the device milliseconds of one count in a burst
+    of `burst` counts (CUDA events on the current stream), and the count."""
+    import torch
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    st = torch.cuda.current_stream()
+    g.tc_async(variant, st.cuda_stream, out.data_ptr())
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(burst):
+            g.tc_async(variant, st.cuda_stream, out.data_ptr())
+        e1.record(st)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) / burst)
+    return float(np.median(ts)), int(out.item())
+
+
+def sched_eval(g):
+    """Triangle-count schedules of one oriented graph, in device ms: the
+    fixed rule, the shipped learned scheduler, the per-task optimum of the
+    logged costs (each owner in its cheapest of the 6 configurations) and
+    the reference-threshold hash kernel (plain heuristic) on the graph and
+    on its degree-relabelled copy (the reference's v-centric input)."""
+    res = {}
+    res["fixed_ms"], want = count_ms(g, gpm.TC_BITMAP)
+    gpm.Sched.pretrained().attach(g)
+    res["learned_ms"], c = count_ms(g, gpm.TC_LEARNED)
+    assert c == want
+    cost = g.task_costs()
+    task = cost.sum(axis=1) > 0
+    best = np.argmin(np.where(cost > 0, cost, np.inf), axis=1).astype(np.uint8)
+    best[~task] = 1
+    res["logged_warp_cycles_per_task_optimum"] = float(np.min(np.where(cost > 0, cost, np.inf), axis=1)[task].sum())
+    g.set_schedule(best)
+    res["per_task_optimum_ms"], c = count_ms(g, gpm.TC_LEARNED)
+    assert c == want
+    cta = np.argmin(np.where(cost[:, 3:] > 0, cost[:, 3:], np.inf), axis=1).astype(np.uint8) + 3
+    cta[~task] = 4
+    g.set_schedule(cta)
+    res["per_task_optimum_cta_only_ms"], c = count_ms(g, gpm.TC_LEARNED)
+    assert c == want
+    res["plain_hash_ms"], c = count_ms(g, gpm.TC_HASH, reps=3, burst=2)
+    assert c == want
+    res["triangles"] = want
+    return res
+
+
+def run_sched(scales=(18, 20, 22)):
+    res = {"workload": "tc_schedules"}
+    for sc in scales:
+        g = gpm.Graph.rmat(sc, 16, seed=1).orient()
+        res[f"rmat{sc}"] = sched_eval(g)
+        r = gpm.Graph.rmat(sc, 16, seed=1).orient(relabel=True)
+        res[f"rmat{sc}"]["plain_hash_relabelled_ms"], _ = count_ms(r, gpm.TC_HASH, reps=3, burst=2)
+        print(json.dumps({sc: res[f"rmat{sc}"]}), flush=True)
+    n, s, d = gpm.gen_chung_lu(1000000, 2.1, 32.0, seed=7)
+    g = gpm.Graph.from_edges(n, s, d).orient()
+    res["chunglu_1e6_g2.1_d32"] = sched_eval(g)
+    return res
+
+
 def run_clique(scale):
     g = gpm.Graph.rmat(scale, 16, seed=1).orient()
     res = {"workload": f"clique_rmat{scale}_ef16"}
@@ -184,7 +248,7 @@ def run_batch(count, nmax):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", default="er,clique,motif,motifcl,match,batch")
+    ap.add_argument("--only", default="er,clique,motif,motifcl,match,batch,sched")
     ap.add_argument("--quick", action="store_true", help="smaller sizes for a smoke run")
     ap.add_argument("--match-scales", default="", help="e.g. 16,18,20,21: the labelled workload at growing scales")
     ap.add_argument("--match-budget", type=float, default=240.0, help="seconds a query may take at its last scale x 8")
@@ -206,6 +270,8 @@ def main():
             print(json.dumps(run_match(12 if a.quick else 16)), flush=True)
     if "batch" in todo:
         print(json.dumps(run_batch(32 if a.quick else 256, 3e4 if a.quick else 1e6)), flush=True)
+    if "sched" in todo:
+        print(json.dumps(run_sched((14, 16) if a.quick else (18, 20, 22))), flush=True)
 
 
 if __name__ == "__main__":

@@ -277,6 +277,15 @@ int gpm_sched_attach(gpm_graph *g, gpm_sched *s);
 int gpm_sched_set_default(gpm_sched *s);
 /* The configuration the scheduler gives each vertex's task (255: no task). */
 int gpm_sched_assign(gpm_sched *s, gpm_graph *g, uint8_t *cfg);
+/* The logged cost (active warp-cycles) of every owner task of g under each
+ * of the 6 configurations: cost[6 * v + c] (host, 6 * n floats; 0 for
+ * vertices that own no task).  The instrumented runs behind the training data
+ * of gpm_sched_collect, per vertex. */
+int gpm_tc_task_costs(gpm_graph *g, float *cost);
+/* Fixes the per-owner configuration GPM_TC_LEARNED runs on g (host cfg[v] in
+ * 0..5, one byte per vertex), e.g. the per-task optimum of gpm_tc_task_costs:
+ * it replaces the scheduler's choice until the graph's plans are dropped. */
+int gpm_tc_set_schedule(gpm_graph *g, const uint8_t *cfg);
 
 /* ---- batches of graphs (no reference counterpart: the reference runs one
  * solver per graph and synchronises after every kernel,

@@ -1,8 +1,8 @@
 """Counts of the reference's own sub_ceci matcher on the labelled workload's
 graphs, as a golden fixture.
 
-    python tests/golden/make_ceci_config_golden.py [--scales 16,18,21] [--workdir DIR]
-                                                   [--timeout 7200] [--jobs 4]
+    python tests/golden/make_ceci_config_golden.py [--scales 16,18,21] [--queries 21:triangle,cycle4,diamond]
+                                                   [--workdir DIR] [--timeout 7200] [--jobs 4]
 
 sub_ceci is built from the reference's sources into oracle/_ref/myceci
 (`make -C oracle ref`).  For each R-MAT scale (edge factor 16, seed 3, 8
@@ -14,7 +14,8 @@ runs
 
     myceci -d data.graph -q <query>.graph -filter CECI -order CECI -engine CECI
 
-for every query, --jobs at a time, each for at most --timeout seconds.  A
+for every query (at the scales --queries names, only the queries it lists),
+--jobs at a time, each for at most --timeout seconds.  A
 query's output already present in the work directory from an earlier run of
 the same command on the same files is read instead of run again (the R-MAT 21
 4-cycle and diamond take sub_ceci about an hour each).  ceci_config.npz keeps
@@ -67,16 +68,19 @@ def run_one(d, name, timeout):
     if got:
         return got
     t0 = time.time()
+    # sub_ceci prints two lines per search call (gigabytes on these graphs):
+    # only the summary at the end is kept
     with open(out, "w") as f:
-        try:
-            subprocess.run([MYCECI, "-d", os.path.join(d, "data.graph"), "-q", os.path.join(d, name + ".graph"),
-                            "-filter", "CECI", "-order", "CECI", "-engine", "CECI"], stdout=f,
-                           stderr=subprocess.STDOUT, timeout=timeout, check=True)
-        except subprocess.TimeoutExpired:
-            print(f"{d} {name}: no result within {timeout} s", flush=True)
-            return None
-    print(f"{d} {name}: {time.time() - t0:.0f} s", flush=True)
-    return parse(out)
+        p1 = subprocess.Popen(["timeout", str(int(timeout)), MYCECI, "-d", os.path.join(d, "data.graph"), "-q",
+                               os.path.join(d, name + ".graph"), "-filter", "CECI", "-order", "CECI", "-engine",
+                               "CECI"], stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+        p2 = subprocess.Popen(["tail", "-n", "40"], stdin=p1.stdout, stdout=f)
+        p1.stdout.close()
+        p2.wait()
+        p1.wait()
+    got = parse(out)
+    print(f"{d} {name}: {time.time() - t0:.0f} s, {'done' if got else 'no result (time limit)'}", flush=True)
+    return got
 
 
 def main():
@@ -85,7 +89,10 @@ def main():
     ap.add_argument("--workdir", default=os.path.join(ROOT, "_work", "ceci"))
     ap.add_argument("--timeout", type=float, default=7200)
     ap.add_argument("--jobs", type=int, default=4)
+    ap.add_argument("--queries", default="21:triangle,cycle4,diamond",
+                    help="scale:q1,q2;scale:... -- queries run at that scale (default: all five)")
     a = ap.parse_args()
+    only = {int(t.split(":")[0]): t.split(":")[1].split(",") for t in a.queries.split(";") if t}
     names = list(W.SHAPES)
     rows = {}
     if os.path.exists(OUT):
@@ -108,7 +115,8 @@ def main():
             if os.path.exists(qp) and open(qp).read() != open(fresh).read():
                 os.remove(os.path.join(d, name + ".out")) if os.path.exists(os.path.join(d, name + ".out")) else None
             os.replace(fresh, qp)
-            jobs.append((scale, qi, d, name, ql))
+            if scale not in only or name in only[scale]:
+                jobs.append((scale, qi, d, name, ql))
     with ThreadPoolExecutor(a.jobs) as pool:
         res = list(pool.map(lambda j: run_one(j[2], j[3], a.timeout), jobs))
     for (scale, qi, d, name, ql), got in zip(jobs, res):

@@ -53,6 +53,7 @@ def test_tc_rmat22_equals_reference_solvers():
     want = int(z["tc_e_centric"])
     assert want == int(z["tc_v_centric"])
     g = rmat_graph(z, "tc", W.TC_SEED).orient()
+    gpm.Sched.pretrained().attach(g)  # the shipped weights drive TC_LEARNED
     out = np.zeros(1, np.uint64)
     import torch
     d = torch.zeros(1, dtype=torch.int64, device="cuda")
