@@ -153,13 +153,14 @@ class Clocks:
 
 def profiled(name, key):
     """A figure recorded in a committed ncu summary (profiles/<name>.md, a
-    line '<key>: <int>'), else None."""
+    line '<key>: <number>'), else None."""
     path = os.path.join(ROOT, "profiles", name + ".md")
     if not os.path.exists(path):
         return None
     for line in open(path):
         if line.strip().startswith(key + ":"):
-            return int(line.split(":", 1)[1].strip())
+            v = line.split(":", 1)[1].strip()
+            return float(v) if "." in v else int(v)
     return None
 
 
@@ -507,7 +508,11 @@ def clique_workload(args, stream):
         r = {"cliques": c, "value": c / (avg / 1e3), "ms_per_count": avg, "steps": reps,
              "ms_first_call": first[0],
              "roofline": roofline(profiled(f"k_clique_local_rmat{W.CLIQUE_SCALE}",
-                                           f"traffic_bytes_per_launch[k{k}]"), avg, hbm, peak_kind)}
+                                           f"traffic_bytes_per_launch[k{k}]"), avg, hbm, peak_kind,
+                                  issue_active_pct=profiled(f"k_clique_local_rmat{W.CLIQUE_SCALE}",
+                                                            f"issue_active_pct[k{k}]"),
+                                  note="bitset intersections in shared memory: issue-bound, DRAM only for "
+                                       "the graph (profiles/k_clique_local_rmat20.md)")}
         if k == 4:
             # the reference-shaped path: warp per stored edge, materialised
             # nested intersections (clique_4_edge_warp)
@@ -620,8 +625,11 @@ def motif_workload(args, stream):
         "e2e": {"value": total / (min(e2e_ms) / 1e3), "unit": "instances/s", "ms_per_step": min(e2e_ms),
                 "h2d_bytes_per_step": int(hsrc.numel() * 4 + hdst.numel() * 4),
                 "d2h_bytes_per_step": int(8 * 8 * ng)},
-        "roofline": roofline(profiled("k_c4_big_chunglu200k", "traffic_bytes_per_launch[batch256]"), avg,
-                             hbm, peak_kind),
+        "roofline": roofline(profiled("k_edge_tri_batch32", "traffic_bytes_per_launch[c4_big_batch256]"),
+                             stages["four_cycles"], hbm, peak_kind, kernel="k_c4_big (the 4-cycle stage)",
+                             issue_active_pct=profiled("k_edge_tri_batch32", "issue_active_pct[edge_tri_batch32]"),
+                             note="the dominant stage's kernel; the pipeline is issue- and latency-bound "
+                                  "(profiles/k_edge_tri_batch32.md, profiles/k_c4_big_chunglu200k.md)"),
         "gpu_launches_timed": None,
     })
     if not args.no_cpu:
@@ -661,7 +669,31 @@ def match_workload(args, stream):
         tot_e += c
         tot_ms += avg
     res["value"] = tot_e / (tot_ms / 1e3) if tot_ms else None
+    res["ms_per_step"] = tot_ms
     res["untimed_queries"] = [q for q in queries if q not in todo]
+    hbm, peak_kind = peaks()
+    if "cycle4" in res["queries"]:
+        res["roofline"] = roofline(profiled("k_match_rmat21_cycle4", "traffic_bytes_per_launch[cycle4_rmat21]"),
+                                   res["queries"]["cycle4"]["ms"], hbm, peak_kind, kernel="k_match (4-cycle query)",
+                                   issue_active_pct=profiled("k_match_rmat18_cycle4", "issue_active_pct[cycle4_rmat18]"),
+                                   note="load-latency-bound back-edge tests, 95 % L2 hits "
+                                        "(profiles/k_match_rmat18_cycle4.md)")
+    if todo:
+        # the same queries counted together: one persistent launch over every
+        # query's tasks, autotuned task split, CUDA-graph replay -- against
+        # one gpm_match call per query (each synchronising, as the reference
+        # synchronises after every pattern)
+        qs = [gpm.Query(*[queries[k][0], queries[k][1][:, 0], queries[k][1][:, 1], queries[k][2]]) for k in todo]
+        mb = gpm.MatchBatch(g, qs)
+        span = mb.autotune()
+        first, r = event_ms(lambda: mb.run(use_graph=True), stream)
+        reps = max(1, min(args.steps, 3))
+        ms, r = event_ms(lambda: mb.run(use_graph=True), stream, reps)
+        assert r[:, 0].tolist() == [res["queries"][k]["embeddings"] for k in todo]
+        bt = sum(ms) / len(ms)
+        res["batched"] = {"queries": todo, "ms_per_replay": bt, "value": tot_e / (bt / 1e3), "tuned_span": span,
+                          "tasks": mb.info()[0], "speedup_vs_single_calls": tot_ms / bt, "steps": reps}
+        mb.close()
     if not args.no_e2e and todo:
         # end to end: host edge list + labels -> graph on the device -> label
         # partition -> the first query's count -> result

@@ -123,21 +123,32 @@ __device__ __forceinline__ bool adjacent(const HubIndex &hub, const int64_t *__r
 // position n-2 at once, the last vertex's candidate segments (each y's
 // shortest) are laid end to end and every lane takes one entry of the
 // concatenation, so short segments do not leave lanes idle.
-// TRACK: every embedding found takes a slot of *found; those below `limit`
-// are written to emb_out (when given: q.n data-vertex ids per embedding, in
-// query-vertex order), and the whole grid stops once `limit` are found
-// (sub_ceci's -num, myceci.cpp:615-617).  Otherwise the count goes to *out.
 constexpr int kMatchWarps = 8;
+struct MatchGraph {
+  const int64_t *off;
+  const int32_t *adj, *ladj, *loff, *labels;
+  int L;
+  HubIndex hub;
+};
+
+// The embeddings of one (root, second vertex) task, by one warp; lane 0
+// returns the count (TRACK: counted into *found instead, see k_match).
+// chunk >= 0 restricts position 2's candidates to the `span` entries from
+// `chunk` on (tasks split by the batch path); buf is the warp's shared
+// buffer of kMaxQ - 2 rows of 32 candidates.
 template <bool TRACK>
-__global__ void __launch_bounds__(kMatchWarps * 32)
-    k_match(QueryPlan q, const int2 *__restrict__ pairs, int64_t n, const int64_t *__restrict__ off,
-            const int32_t *__restrict__ adj, const int32_t *__restrict__ ladj, const int32_t *__restrict__ loff,
-            int L, const int32_t *__restrict__ labels, HubIndex hub, unsigned long long *__restrict__ cursor,
-            unsigned long long *__restrict__ out, unsigned long long limit, unsigned long long *found,
-            int32_t *__restrict__ emb_out) {
-  __shared__ int32_t sbuf[kMatchWarps][kMaxQ - 2][32];
+__device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, const MatchGraph &G, int32_t root,
+                                                         int32_t second, int64_t chunk, int64_t span,
+                                                         int32_t (*buf)[32], unsigned long long limit,
+                                                         unsigned long long *found, int32_t *__restrict__ emb_out) {
+  const int64_t *__restrict__ off = G.off;
+  const int32_t *__restrict__ adj = G.adj;
+  const int32_t *__restrict__ ladj = G.ladj;
+  const int32_t *__restrict__ loff = G.loff;
+  const int32_t *__restrict__ labels = G.labels;
+  const int L = G.L;
+  const HubIndex &hub = G.hub;
   const unsigned lane = lane_id();
-  int32_t(*buf)[32] = sbuf[threadIdx.x >> 5];
   int32_t emb[kMaxQ] = {};
   int64_t pos[kMaxQ], end[kMaxQ];
   uint32_t chk[kMaxQ];
@@ -260,6 +271,61 @@ __global__ void __launch_bounds__(kMatchWarps * 32)
     }
   };
 
+  emb[0] = root;
+  emb[1] = second;
+  if (pre == 1) {  // three query vertices: the pair's second vertex is position n-2
+    close(second, 1);
+    return c;
+  }
+  int d = 2;
+  open(2);
+  if (chunk >= 0) {
+    pos[2] += chunk;
+    end[2] = min(end[2], pos[2] + span);
+  }
+  bcnt[2] = bcur[2] = 0;
+  while (d >= 2) {
+    if (TRACK && *(volatile unsigned long long *)found >= limit) break;
+    if (d == pre) {
+      if (pos[d] >= end[d]) {
+        --d;
+        continue;
+      }
+      const int k = fill(d);
+      if (k) close((int)lane < k ? buf[d - 2][lane] : 0, k);
+      continue;
+    }
+    if (bcur[d] < bcnt[d]) {
+      emb[d] = buf[d - 2][bcur[d]++];
+      ++d;
+      open(d);
+      bcnt[d] = bcur[d] = 0;
+      continue;
+    }
+    if (pos[d] < end[d]) {
+      bcnt[d] = fill(d);
+      bcur[d] = 0;
+      continue;
+    }
+    --d;
+  }
+  return c;
+}
+
+// One query over its (root, second vertex) pairs, drained from an atomic
+// cursor by a persistent grid.  TRACK: every embedding found takes a slot of
+// *found; those below `limit` are written to emb_out (when given: q.n
+// data-vertex ids per embedding, in query-vertex order), and the whole grid
+// stops once `limit` are found (sub_ceci's -num, myceci.cpp:615-617).
+// Otherwise the count goes to *out.
+template <bool TRACK>
+__global__ void __launch_bounds__(kMatchWarps * 32)
+    k_match(QueryPlan q, MatchGraph G, const int2 *__restrict__ pairs, int64_t n,
+            unsigned long long *__restrict__ cursor, unsigned long long *__restrict__ out, unsigned long long limit,
+            unsigned long long *found, int32_t *__restrict__ emb_out) {
+  __shared__ int32_t sbuf[kMatchWarps][kMaxQ - 2][32];
+  const unsigned lane = lane_id();
+  unsigned long long c = 0;
   while (true) {
     unsigned long long r = 0;
     if (lane == 0) r = atomicAdd(cursor, 1ull);
@@ -267,40 +333,7 @@ __global__ void __launch_bounds__(kMatchWarps * 32)
     if (r >= (unsigned long long)n) break;
     if (TRACK && *(volatile unsigned long long *)found >= limit) break;
     const int2 pr = pairs[r];
-    emb[0] = pr.x;
-    emb[1] = pr.y;
-    if (pre == 1) {  // three query vertices: the pair's second vertex is position n-2
-      close(pr.y, 1);
-      continue;
-    }
-    int d = 2;
-    open(2);
-    bcnt[2] = bcur[2] = 0;
-    while (d >= 2) {
-      if (TRACK && *(volatile unsigned long long *)found >= limit) break;
-      if (d == pre) {
-        if (pos[d] >= end[d]) {
-          --d;
-          continue;
-        }
-        const int k = fill(d);
-        if (k) close((int)lane < k ? buf[d - 2][lane] : 0, k);
-        continue;
-      }
-      if (bcur[d] < bcnt[d]) {
-        emb[d] = buf[d - 2][bcur[d]++];
-        ++d;
-        open(d);
-        bcnt[d] = bcur[d] = 0;
-        continue;
-      }
-      if (pos[d] < end[d]) {
-        bcnt[d] = fill(d);
-        bcur[d] = 0;
-        continue;
-      }
-      --d;
-    }
+    c += match_task<TRACK>(q, G, pr.x, pr.y, -1, 0, sbuf[threadIdx.x >> 5], limit, found, emb_out);
   }
   if (TRACK) return;
   c = warp_sum(c);
@@ -709,13 +742,12 @@ static int match_run(gpm_graph *g, const gpm_query *q, unsigned long long limit,
   GPM_TRY(cursor.reserve(1));
   GPM_CUDA(cudaMemset(cursor.p, 0, 8));
   GPM_CUDA(cudaMemset(d.p, 0, 8));
+  const MatchGraph G{g->off.p, g->adj.p, lc->ladj.p, lc->loff.p, g->labels.p, lc->L, hub};
   if (track)
-    k_match<true><<<grid, kMatchWarps * 32>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p, lc->loff.p,
-                                              lc->L, g->labels.p, hub, cursor.p, d.p, limit, found.p,
+    k_match<true><<<grid, kMatchWarps * 32>>>(plan, G, pairs.p, (int64_t)np, cursor.p, d.p, limit, found.p,
                                               emb ? demb.p : nullptr);
   else
-    k_match<false><<<grid, kMatchWarps * 32>>>(plan, pairs.p, (int64_t)np, g->off.p, g->adj.p, lc->ladj.p,
-                                               lc->loff.p, lc->L, g->labels.p, hub, cursor.p, d.p, limit, found.p,
+    k_match<false><<<grid, kMatchWarps * 32>>>(plan, G, pairs.p, (int64_t)np, cursor.p, d.p, limit, found.p,
                                                nullptr);
   GPM_LAUNCH_CHECK();
   unsigned long long h = 0;
@@ -736,6 +768,361 @@ int gpm_match_limit(gpm_graph *g, const gpm_query *q, uint64_t limit, uint64_t *
 int gpm_match_list(gpm_graph *g, const gpm_query *q, uint64_t limit, int32_t *emb, uint64_t *written) {
   if (!emb && limit > 0) return fail(GPM_EINVAL, "gpm_match_list: NULL output");
   return match_run(g, q, limit, emb, written);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Many labelled queries on one data graph in one persistent launch.
+//
+// The reference runs one kernel per pattern and synchronises after each
+// (src/PatternSolver.cuh:177-246).  Here the (root, second vertex) pairs of
+// every query become one task list, each task carrying its query; a warp
+// loads its task's plan into shared memory and walks the task with the same
+// depth-first code as gpm_match, so the GPU stays busy across query
+// boundaries and no query waits for another's tail.  Tasks of 4+ vertex
+// queries can be split over chunks of position 2's candidates (the span
+// chosen by gpm_match_batch_autotune) so hub tasks do not form the tail.
+// With a member id per vertex (many graphs as one disjoint union), each
+// embedding is counted for its root's member.  The launch (cursor reset,
+// count reset, kernel) is captured into a CUDA graph and replayed.
+// ---------------------------------------------------------------------------
+struct gpm_match_batch {
+  gpm_graph *g = nullptr;
+  int nq = 0, nm = 1;
+  std::vector<gpm::QueryPlan> plans;
+  std::vector<gpm::DevBuf<int2>> pairs;  // per query (empty for 1- and 2-vertex queries)
+  std::vector<int64_t> npairs;
+  gpm::DevBuf<gpm::QueryPlan> dplans;
+  gpm::DevBuf<int32_t> member;           // n (nm > 1 only)
+  gpm::DevBuf<unsigned long long> base;  // counts of 1- and 2-vertex queries, nq * nm
+  gpm::DevBuf<unsigned long long> out, cursor;
+  gpm::DevBuf<int4> tasks;
+  int64_t ntasks = 0, span = 0;
+  int grid = 0;  // persistent grid of k_match_batch
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~gpm_match_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+namespace gpm {
+
+__global__ void __launch_bounds__(kMatchWarps * 32)
+    k_match_batch(const QueryPlan *__restrict__ plans, MatchGraph G, const int4 *__restrict__ tasks, int64_t ntasks,
+                  int64_t span, const int32_t *__restrict__ member, int nm, unsigned long long *__restrict__ cursor,
+                  unsigned long long *__restrict__ out) {
+  __shared__ int32_t sbuf[kMatchWarps][kMaxQ - 2][32];
+  __shared__ QueryPlan splan[kMatchWarps];
+  static_assert(sizeof(QueryPlan) % 4 == 0, "plan copied as words");
+  const int w = threadIdx.x >> 5;
+  const unsigned lane = lane_id();
+  int cur = -1;
+  while (true) {
+    unsigned long long r = 0;
+    if (lane == 0) r = atomicAdd(cursor, 1ull);
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if (r >= (unsigned long long)ntasks) break;
+    const int4 t = tasks[r];
+    if (t.z != cur) {
+      __syncwarp();
+      const int32_t *src = reinterpret_cast<const int32_t *>(plans + t.z);
+      int32_t *dst = reinterpret_cast<int32_t *>(&splan[w]);
+      for (int i = lane; i < (int)(sizeof(QueryPlan) / 4); i += 32) dst[i] = src[i];
+      __syncwarp();
+      cur = t.z;
+    }
+    const unsigned long long c = match_task<false>(splan[w], G, t.x, t.y, t.w < 0 ? -1 : (int64_t)t.w * span, span,
+                                                   sbuf[w], ~0ull, nullptr, nullptr);
+    if (lane == 0 && c) atomicAdd(&out[(int64_t)t.z * nm + (member ? member[t.x] : 0)], c);
+  }
+}
+
+// Position 2's candidate count of each pair (the shortest label segment among
+// its mapped query-neighbours, as match_task opens it), as the task count of
+// the pair: ceil(len / span), at least 1.
+__global__ void k_pair_tasks(QueryPlan q, const int2 *__restrict__ pairs, int64_t np, const int64_t *__restrict__ off,
+                             const int32_t *__restrict__ loff, int L, int64_t span, int64_t *__restrict__ cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t e[2] = {pairs[i].x, pairs[i].y};
+    const int lab = q.label[2];
+    int64_t best = -1;
+    const uint32_t nb = q.back_pos[2] | (1u << q.parent_pos[2]);
+    for (uint32_t bm = nb; bm; bm &= bm - 1) {
+      const int j = __ffs(bm) - 1;
+      int64_t s, en;
+      seg_range(off, loff, L, e[j], lab, &s, &en);
+      if (best < 0 || en - s < best) best = en - s;
+    }
+    cnt[i] = span > 0 ? max((int64_t)1, (best + span - 1) / span) : 1;
+  }
+}
+__global__ void k_expand_tasks(const int2 *__restrict__ pairs, int64_t np, const int64_t *__restrict__ first,
+                               const int64_t *__restrict__ cnt, int query, int split, int4 *__restrict__ tasks) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t c = 0; c < cnt[i]; ++c)
+      tasks[first[i] + c] = make_int4(pairs[i].x, pairs[i].y, query, split ? (int)c : -1);
+}
+// per-member counts of a one-vertex query (vertices with its label) or of a
+// two-vertex query (its pairs, by the root's member)
+__global__ void k_small_counts(int64_t n, const int32_t *__restrict__ labels, int label, const int2 *__restrict__ pairs,
+                               int64_t np, const int32_t *__restrict__ member, unsigned long long *__restrict__ dst) {
+  const int64_t tot = pairs ? np : n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    if (pairs) atomicAdd(&dst[member ? member[pairs[i].x] : 0], 1ull);
+    else if (labels[i] == label) atomicAdd(&dst[member ? member[i] : 0], 1ull);
+  }
+}
+
+static int label_freq(gpm_graph *g, int maxl, std::vector<int64_t> &freq) {
+  freq.assign(maxl, 0);
+  DevBuf<unsigned long long> h;
+  GPM_TRY(h.reserve(maxl));
+  GPM_CUDA(cudaMemset(h.p, 0, sizeof(unsigned long long) * maxl));
+  if (g->n > 0)
+    k_label_hist<<<(int)std::min<int64_t>((g->n + 255) / 256, num_sms() * 8), 256>>>(g->n, g->labels.p, maxl, h.p);
+  std::vector<unsigned long long> hh(maxl);
+  GPM_CUDA(cudaMemcpy(hh.data(), h.p, sizeof(unsigned long long) * maxl, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < maxl; ++i) freq[i] = (int64_t)hh[i];
+  return GPM_OK;
+}
+
+static void drop_batch_graph(gpm_match_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+// The task list for a given split span (0: one task per pair).
+static int batch_tasks(gpm_match_batch *b, int64_t span) {
+  gpm_graph *g = b->g;
+  LabelCsr *lc = g->lcsr;
+  std::vector<int64_t> cnt_total(b->nq, 0);
+  std::vector<DevBuf<int64_t>> cnt(b->nq), first(b->nq);
+  int64_t total = 0;
+  const int blocks = num_sms() * 8;
+  for (int k = 0; k < b->nq; ++k) {
+    const int64_t np = b->npairs[k];
+    if (b->plans[k].n < 3 || np == 0) continue;
+    GPM_TRY(cnt[k].reserve(np));
+    GPM_TRY(first[k].reserve(np + 1));
+    if (b->plans[k].n >= 4)
+      k_pair_tasks<<<blocks, 256>>>(b->plans[k], b->pairs[k].p, np, g->off.p, lc->loff.p, lc->L, span, cnt[k].p);
+    else
+      k_pair_tasks<<<blocks, 256>>>(b->plans[k], b->pairs[k].p, np, g->off.p, lc->loff.p, lc->L, 0, cnt[k].p);
+    GPM_LAUNCH_CHECK();
+    size_t tmp = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tmp, cnt[k].p, first[k].p + 1, (int)np);
+    DevBuf<char> t;
+    GPM_TRY(t.reserve(tmp));
+    GPM_CUDA(cudaMemset(first[k].p, 0, sizeof(int64_t)));
+    cub::DeviceScan::InclusiveSum(t.p, tmp, cnt[k].p, first[k].p + 1, (int)np);
+    int64_t c = 0;
+    GPM_CUDA(cudaMemcpy(&c, first[k].p + np, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    cnt_total[k] = c;
+    total += c;
+  }
+  GPM_TRY(b->tasks.reserve(std::max<int64_t>(total, 1)));
+  int64_t at = 0;
+  for (int k = 0; k < b->nq; ++k) {
+    if (!cnt_total[k]) continue;
+    // each query's tasks at its own offset: shift the scan by `at`
+    k_expand_tasks<<<blocks, 256>>>(b->pairs[k].p, b->npairs[k], first[k].p, cnt[k].p, k,
+                                    b->plans[k].n >= 4 && span > 0, b->tasks.p + at);
+    GPM_LAUNCH_CHECK();
+    at += cnt_total[k];
+  }
+  GPM_CUDA(cudaDeviceSynchronize());
+  b->ntasks = total;
+  b->span = span;
+  drop_batch_graph(b);
+  return GPM_OK;
+}
+
+static int batch_grid() {
+  static int grid = 0;
+  if (!grid) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_batch, kMatchWarps * 32, 0);
+    grid = std::max(1, per_sm) * num_sms();
+  }
+  return grid;
+}
+
+static int batch_launch(gpm_match_batch *b, cudaStream_t st) {
+  gpm_graph *g = b->g;
+  LabelCsr *lc = g->lcsr;
+  const size_t bytes = sizeof(unsigned long long) * b->nq * b->nm;
+  GPM_CUDA(cudaMemcpyAsync(b->out.p, b->base.p, bytes, cudaMemcpyDeviceToDevice, st));
+  GPM_CUDA(cudaMemsetAsync(b->cursor.p, 0, 8, st));
+  if (b->ntasks == 0) return GPM_OK;
+  const MatchGraph G{g->off.p, g->adj.p, lc->ladj.p, lc->loff.p, g->labels.p, lc->L,
+                     HubIndex{lc->hub_slot.p, lc->hub_bm.p, lc->hub_words}};
+  k_match_batch<<<b->grid, kMatchWarps * 32, 0, st>>>(b->dplans.p, G, b->tasks.p, b->ntasks, b->span,
+                                                                 b->nm > 1 ? b->member.p : nullptr, b->nm, b->cursor.p,
+                                                                 b->out.p);
+  GPM_LAUNCH_CHECK();
+  return GPM_OK;
+}
+
+static int batch_run(gpm_match_batch *b, int use_graph, cudaStream_t st) {
+  if (!use_graph) return batch_launch(b, st);
+  if (!b->exec) {
+    // capture on a private stream so the caller's stream may be the legacy one
+    cudaStream_t cs;
+    GPM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    int s = e == cudaSuccess ? batch_launch(b, cs) : fail(GPM_ECUDA, cudaGetErrorString(e));
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    if (s != GPM_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return s;
+    }
+    if (e != cudaSuccess) return fail(GPM_ECUDA, std::string("match batch capture: ") + cudaGetErrorString(e));
+    b->graph = graph;
+    GPM_CUDA(cudaGraphInstantiate(&b->exec, graph, 0));
+  }
+  GPM_CUDA(cudaGraphLaunch(b->exec, st));
+  return GPM_OK;
+}
+
+}  // namespace gpm
+
+extern "C" {
+
+int gpm_match_batch_create(gpm_graph *g, int nq, const gpm_query *const *queries, const int32_t *member,
+                           int nmembers, gpm_match_batch **out) {
+  if (!g || !out || nq < 1 || !queries || (member && nmembers < 1))
+    return fail(GPM_EINVAL, "gpm_match_batch_create: bad argument");
+  if (!g->labels.p) return fail(GPM_EINVAL, "the data graph carries no labels");
+  if (g->oriented) return fail(GPM_EINVAL, "matching needs the symmetric (unoriented) data graph");
+  for (int k = 0; k < nq; ++k)
+    if (!queries[k]) return fail(GPM_EINVAL, "gpm_match_batch_create: NULL query");
+  auto *b = new gpm_match_batch();
+  b->g = g;
+  b->nq = nq;
+  b->nm = member ? nmembers : 1;
+  auto bail = [&](int s) {
+    delete b;
+    return s;
+  };
+  int s;
+  if (member) {
+    for (int64_t v = 0; v < g->n; ++v)
+      if (member[v] < 0 || member[v] >= nmembers) return bail(fail(GPM_EINVAL, "member id out of range"));
+    if ((s = b->member.reserve(std::max<int64_t>(g->n, 1)))) return bail(s);
+    if (g->n && cudaMemcpy(b->member.p, member, sizeof(int32_t) * g->n, cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(GPM_ECUDA, "member upload"));
+  }
+  int maxl = 1;
+  for (int k = 0; k < nq; ++k)
+    for (int i = 0; i < queries[k]->n; ++i) maxl = std::max(maxl, queries[k]->labels[i] + 1);
+  std::vector<int64_t> freq;
+  if ((s = label_freq(g, maxl, freq))) return bail(s);
+  if ((s = ensure_label_csr(g))) return bail(s);
+  LabelCsr *lc = g->lcsr;
+  const size_t cells = (size_t)nq * b->nm;
+  if ((s = b->base.reserve(cells)) || (s = b->out.reserve(cells)) || (s = b->cursor.reserve(1)) ||
+      (s = b->dplans.reserve(nq)))
+    return bail(s);
+  GPM_CUDA(cudaMemset(b->base.p, 0, sizeof(unsigned long long) * cells));
+  b->plans.resize(nq);
+  b->pairs.resize(nq);
+  b->npairs.assign(nq, 0);
+  DevBuf<unsigned long long> np;
+  if ((s = np.reserve(1))) return bail(s);
+  const int blocks = (int)std::min<int64_t>((g->n * 32 + 255) / 256, (int64_t)num_sms() * 16);
+  const int sblocks = (int)std::min<int64_t>((g->n + 255) / 256 + 1, (int64_t)num_sms() * 8);
+  for (int k = 0; k < nq; ++k) {
+    QueryPlan &p = b->plans[k];
+    if ((s = plan_query(queries[k], freq, &p))) return bail(s);
+    if (p.n == 1) {
+      if (g->n) k_small_counts<<<sblocks, 256>>>(g->n, g->labels.p, p.label[0], nullptr, 0,
+                                                  b->nm > 1 ? b->member.p : nullptr, b->base.p + (size_t)k * b->nm);
+      continue;
+    }
+    GPM_CUDA(cudaMemset(np.p, 0, 8));
+    k_match_pairs<<<blocks, 256>>>(p, g->n, g->off.p, lc->ladj.p, lc->loff.p, lc->L, g->labels.p, 1, nullptr, np.p);
+    unsigned long long h = 0;
+    GPM_CUDA(cudaMemcpy(&h, np.p, 8, cudaMemcpyDeviceToHost));
+    b->npairs[k] = (int64_t)h;
+    if (h == 0) continue;
+    if ((s = b->pairs[k].reserve(h))) return bail(s);
+    GPM_CUDA(cudaMemset(np.p, 0, 8));
+    k_match_pairs<<<blocks, 256>>>(p, g->n, g->off.p, lc->ladj.p, lc->loff.p, lc->L, g->labels.p, 0, b->pairs[k].p,
+                                   np.p);
+    if (p.n == 2)
+      k_small_counts<<<sblocks, 256>>>(0, nullptr, 0, b->pairs[k].p, (int64_t)h, b->nm > 1 ? b->member.p : nullptr,
+                                       b->base.p + (size_t)k * b->nm);
+  }
+  GPM_CUDA(cudaMemcpy(b->dplans.p, b->plans.data(), sizeof(QueryPlan) * nq, cudaMemcpyHostToDevice));
+  b->grid = batch_grid();
+  if ((s = batch_tasks(b, 0))) return bail(s);
+  *out = b;
+  return GPM_OK;
+}
+
+int gpm_match_batch_autotune(gpm_match_batch *b, int64_t *span) {
+  if (!b) return fail(GPM_EINVAL, "NULL batch");
+  static const int64_t cand[] = {0, 16384, 2048, 256};
+  cudaEvent_t e0, e1;
+  GPM_CUDA(cudaEventCreate(&e0));
+  GPM_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int64_t best_span = b->span;
+  for (int64_t c : cand) {
+    GPM_TRY(batch_tasks(b, c));
+    GPM_TRY(batch_launch(b, 0));  // warm-up
+    GPM_CUDA(cudaEventRecord(e0, 0));
+    GPM_TRY(batch_launch(b, 0));
+    GPM_CUDA(cudaEventRecord(e1, 0));
+    GPM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    GPM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) {
+      best = ms;
+      best_span = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  GPM_TRY(batch_tasks(b, best_span));
+  if (span) *span = best_span;
+  return GPM_OK;
+}
+
+int gpm_match_batch_run_async(gpm_match_batch *b, int use_graph, void *stream, uint64_t *d_out) {
+  if (!b || !d_out) return fail(GPM_EINVAL, "gpm_match_batch_run_async: NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  GPM_TRY(batch_run(b, use_graph, st));
+  GPM_CUDA(cudaMemcpyAsync(d_out, b->out.p, sizeof(unsigned long long) * b->nq * b->nm, cudaMemcpyDeviceToDevice, st));
+  return GPM_OK;
+}
+
+int gpm_match_batch_run(gpm_match_batch *b, int use_graph, void *stream, uint64_t *out) {
+  if (!b || !out) return fail(GPM_EINVAL, "gpm_match_batch_run: NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  GPM_TRY(batch_run(b, use_graph, st));
+  GPM_CUDA(cudaMemcpyAsync(out, b->out.p, sizeof(unsigned long long) * b->nq * b->nm, cudaMemcpyDeviceToHost, st));
+  GPM_CUDA(cudaStreamSynchronize(st));
+  return GPM_OK;
+}
+
+int gpm_match_batch_info(const gpm_match_batch *b, int64_t *tasks, int64_t *span) {
+  if (!b) return fail(GPM_EINVAL, "NULL batch");
+  if (tasks) *tasks = b->ntasks;
+  if (span) *span = b->span;
+  return GPM_OK;
+}
+
+int gpm_match_batch_destroy(gpm_match_batch *b) {
+  delete b;
+  return GPM_OK;
 }
 
 }  // extern "C"

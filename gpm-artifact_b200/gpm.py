@@ -103,6 +103,12 @@ _SIGS = {
     "gpm_match": ([_P, _P, POINTER(c_uint64)], c_int),
     "gpm_match_limit": ([_P, _P, c_uint64, POINTER(c_uint64)], c_int),
     "gpm_match_list": ([_P, _P, c_uint64, _P, POINTER(c_uint64)], c_int),
+    "gpm_match_batch_create": ([_P, c_int, _P, _P, c_int, POINTER(c_void_p)], c_int),
+    "gpm_match_batch_autotune": ([_P, POINTER(c_int64)], c_int),
+    "gpm_match_batch_run": ([_P, c_int, _P, _P], c_int),
+    "gpm_match_batch_run_async": ([_P, c_int, _P, _P], c_int),
+    "gpm_match_batch_info": ([_P, POINTER(c_int64), POINTER(c_int64)], c_int),
+    "gpm_match_batch_destroy": ([_P], c_int),
 }
 for _name, (_args, _res) in _SIGS.items():
     if hasattr(lib, _name):
@@ -434,6 +440,7 @@ class Sched:
 
     def attach(self, g: "Graph"):
         check(lib.gpm_sched_attach(g.h, self.h))
+        g._sched = self  # the graph keeps its scheduler alive
 
     _default = None  # the process default, kept alive while it is the default
 
@@ -540,6 +547,45 @@ class Query:
         self.h = None
 
     __del__ = close
+
+
+class MatchBatch:
+    """Many labelled queries on one data graph in one launch (gpm_match_batch)."""
+
+    def __init__(self, g: "Graph", queries, member=None, nmembers=1):
+        self.g, self.queries = g, list(queries)  # kept alive with the batch
+        arr = (c_void_p * len(self.queries))(*[q.h.value for q in self.queries])
+        mem = None if member is None else _i32(member)
+        self.nm = int(nmembers) if member is not None else 1
+        h = c_void_p()
+        check(lib.gpm_match_batch_create(g.h, len(self.queries), arr, _ptr(mem), self.nm, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.gpm_match_batch_destroy(self.h)
+        self.h = None
+
+    __del__ = close
+
+    def autotune(self) -> int:
+        sp = c_int64()
+        check(lib.gpm_match_batch_autotune(self.h, ctypes.byref(sp)))
+        return sp.value
+
+    def info(self):
+        t, sp = c_int64(), c_int64()
+        check(lib.gpm_match_batch_info(self.h, ctypes.byref(t), ctypes.byref(sp)))
+        return t.value, sp.value
+
+    def run(self, use_graph=True, stream_ptr=0):
+        """Counts as uint64[nq, nmembers]."""
+        out = np.zeros(len(self.queries) * self.nm, np.uint64)
+        check(lib.gpm_match_batch_run(self.h, 1 if use_graph else 0, c_void_p(stream_ptr), _ptr(out)))
+        return out.reshape(len(self.queries), self.nm)
+
+    def run_async(self, use_graph, stream_ptr, d_out_ptr):
+        check(lib.gpm_match_batch_run_async(self.h, 1 if use_graph else 0, c_void_p(stream_ptr), c_void_p(d_out_ptr)))
 
 
 def tc_host_csr(offsets, indices, variant=TC_AUTO, stream_ptr=0) -> int:

@@ -189,6 +189,39 @@ def run_match(scale, seed=3):
     return res
 
 
+def run_match_batch(scale, names, seed=3):
+    """The labelled queries of one graph counted together (gpm_match_batch:
+    one persistent launch over every query's tasks, autotuned task split,
+    CUDA-graph replay) against one gpm_match call per query."""
+    n, s, d = gpm.gen_rmat(scale, 16, seed=seed)
+    lab = gpm.gen_zipf_labels(n, 8, 1.2, seed=seed)
+    g = gpm.Graph.from_edges(n, s, d, labels=lab)
+    off, idx = g.csr()
+    allq = walk_queries_dict(off, idx, lab, seed)
+    qs = [allq[k] for k in names]
+    single, t_single = [], 0.0
+    g.match(qs[0])  # label partition and bitmaps built outside the timings
+    for q in qs:
+        c, t = timed(lambda: g.match(q))
+        single.append(c)
+        t_single += t
+    b = gpm.MatchBatch(g, qs)
+    r, t_first = timed(lambda: b.run(use_graph=True))
+    assert r[:, 0].tolist() == single
+    span = b.autotune()
+    b.run(use_graph=True)
+    r, t = timed(lambda: b.run(use_graph=True), 3)
+    assert r[:, 0].tolist() == single
+    return {"workload": f"match_batch_rmat{scale}_ef16_zipf8", "queries": names, "embeddings": single,
+            "s_single_calls": t_single, "s_batched_first": t_first, "s_batched_replay": t, "tuned_span": span,
+            "tasks": b.info()[0], "speedup_vs_single_calls": t_single / t, "embeddings_per_s": sum(single) / t}
+
+
+def walk_queries_dict(off, idx, lab, seed):
+    from workloads import walk_queries
+    return {k: gpm.Query(kk, e[:, 0], e[:, 1], ql) for k, (kk, e, ql) in walk_queries(off, idx, lab, seed).items()}
+
+
 def run_match_scales(scales, budget_s, seed=3):
     """The labelled workload at growing R-MAT scales (same label law, queries
     walked on each graph): a query stops growing once one run took more than
@@ -252,6 +285,7 @@ def main():
     ap.add_argument("--quick", action="store_true", help="smaller sizes for a smoke run")
     ap.add_argument("--match-scales", default="", help="e.g. 16,18,20,21: the labelled workload at growing scales")
     ap.add_argument("--match-budget", type=float, default=240.0, help="seconds a query may take at its last scale x 8")
+    ap.add_argument("--batch-queries", default="triangle,cycle4,diamond", help="queries of the matchbatch workload")
     a = ap.parse_args()
     todo = a.only.split(",")
     if "er" in todo:
@@ -270,6 +304,8 @@ def main():
             print(json.dumps(run_match(12 if a.quick else 16)), flush=True)
     if "batch" in todo:
         print(json.dumps(run_batch(32 if a.quick else 256, 3e4 if a.quick else 1e6)), flush=True)
+    if "matchbatch" in todo:
+        print(json.dumps(run_match_batch(14 if a.quick else 21, a.batch_queries.split(","))), flush=True)
     if "sched" in todo:
         print(json.dumps(run_sched((14, 16) if a.quick else (18, 20, 22))), flush=True)
 

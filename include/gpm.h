@@ -340,6 +340,32 @@ int gpm_match_limit(gpm_graph *data, const gpm_query *q, uint64_t limit, uint64_
  * arbitrary `limit` of them. */
 int gpm_match_list(gpm_graph *data, const gpm_query *q, uint64_t limit, int32_t *emb, uint64_t *written);
 
+/* ---- batches of labelled queries (no reference counterpart: the reference
+ * launches one kernel per pattern and synchronises after each,
+ * src/PatternSolver.cuh:177-246) ------------------------------------------- */
+typedef struct gpm_match_batch gpm_match_batch;
+/* nq queries on one labelled symmetric data graph, counted together in one
+ * persistent launch (sub_ceci semantics, as gpm_match).  member (host, n ids
+ * in [0, nmembers), may be NULL) names each vertex's member when the data
+ * graph is a disjoint union of many graphs: each embedding is counted for its
+ * root's member.  The plan (each query's (root, second vertex) tasks) is
+ * built here; `data` must outlive the batch. */
+int gpm_match_batch_create(gpm_graph *data, int nq, const gpm_query *const *queries, const int32_t *member,
+                           int nmembers, gpm_match_batch **out);
+/* Chooses how finely tasks of queries with 4 or more vertices are split (the
+ * span of position-2 candidates per task; 0 = unsplit) by timing candidates;
+ * *span (may be NULL) receives it. */
+int gpm_match_batch_autotune(gpm_match_batch *b, int64_t *span);
+/* Counts: out[q * nmembers + m] (host, nq * nmembers uint64, nmembers = 1
+ * without member ids).  use_graph != 0 captures the launch into a CUDA graph
+ * on the first call and replays it afterwards. */
+int gpm_match_batch_run(gpm_match_batch *b, int use_graph, void *stream, uint64_t *out);
+/* The same into device memory d_out without host synchronisation. */
+int gpm_match_batch_run_async(gpm_match_batch *b, int use_graph, void *stream, uint64_t *d_out);
+/* Tasks in the launch and the current split span. */
+int gpm_match_batch_info(const gpm_match_batch *b, int64_t *tasks, int64_t *span);
+int gpm_match_batch_destroy(gpm_match_batch *b);
+
 #ifdef __cplusplus
 }
 #endif
