@@ -91,9 +91,6 @@ struct HashTable {
 // over the warps of the executing group (1 warp for warp tasks, the CTA's
 // warps for CTA tasks).  R-MAT 22: half-warps 7.0 ms against 7.6 ms for
 // whole-warp streaming of the same segments.
-#ifndef GPM_TC_PF
-#define GPM_TC_PF 0
-#endif
 template <class T>
 __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__restrict__ radj,
                                                             const longlong2 *__restrict__ pseg, int64_t l0,
@@ -102,7 +99,6 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
   unsigned long long c = 0;
   const unsigned half = lane >> 4, hl = lane & 15;
   int64_t j;
-#if GPM_TC_PF == 0
   for (j = l0 + wid * 2 + half; j < l1; j += nw * 2) {
     const longlong2 sg = pseg[j];
     const int32_t *__restrict__ q = radj + sg.x;
@@ -112,67 +108,13 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
     for (int i = (int)hl; i < len; i += 16) cs += t.hit(__ldg(q + i));
     c += cs;
   }
-#elif GPM_TC_PF == 1
-  // the next segment's descriptor is loaded before the current one streams
-  const int64_t stride = (int64_t)nw * 2;
-  j = l0 + wid * 2 + half;
-  longlong2 sg = j < l1 ? pseg[j] : make_longlong2(0, 0);
-  for (; j < l1; j += stride) {
-    const longlong2 nx = j + stride < l1 ? pseg[j + stride] : make_longlong2(0, 0);
-    const int32_t *__restrict__ q = radj + sg.x;
-    const int len = (int)(sg.y - sg.x);
-    unsigned cs = 0;
-#pragma unroll 4
-    for (int i = (int)hl; i < len; i += 16) cs += t.hit(__ldg(q + i));
-    c += cs;
-    sg = nx;
-  }
-#else
-  // two segments per half-warp streamed side by side, descriptors ahead
-  const int64_t stride = (int64_t)nw * 2;
-  j = l0 + wid * 2 + half;
-  longlong2 a = j < l1 ? pseg[j] : make_longlong2(0, 0);
-  longlong2 b = j + stride < l1 ? pseg[j + stride] : make_longlong2(0, 0);
-  for (; j < l1; j += 2 * stride) {
-    const longlong2 na = j + 2 * stride < l1 ? pseg[j + 2 * stride] : make_longlong2(0, 0);
-    const longlong2 nb = j + 3 * stride < l1 ? pseg[j + 3 * stride] : make_longlong2(0, 0);
-    const int32_t *__restrict__ qa = radj + a.x;
-    const int32_t *__restrict__ qb = radj + b.x;
-    const int la = (int)(a.y - a.x), lb = (int)(b.y - b.x);
-    const int lm = max(la, lb);
-    unsigned cs = 0;
-#pragma unroll 2
-    for (int i = (int)hl; i < lm; i += 16) {
-      if (i < la) cs += t.hit(__ldg(qa + i));
-      if (i < lb) cs += t.hit(__ldg(qb + i));
-    }
-    c += cs;
-    a = na;
-    b = nb;
-  }
-#endif
   const unsigned grp = lane >> 3, gl = lane & 7;
-#if GPM_TC_PF == 0
   for (j = s0 + wid * 4 + grp; j < s1; j += nw * 4) {
     const longlong2 sg = pseg[j];
     unsigned cs = 0;
     for (int64_t k = sg.x + gl; k < sg.y; k += 8) cs += t.hit(__ldg(radj + k));
     c += cs;
   }
-#else
-  {
-    const int64_t stride4 = (int64_t)nw * 4;
-    j = s0 + wid * 4 + grp;
-    longlong2 sg = j < s1 ? pseg[j] : make_longlong2(0, 0);
-    for (; j < s1; j += stride4) {
-      const longlong2 nx = j + stride4 < s1 ? pseg[j + stride4] : make_longlong2(0, 0);
-      unsigned cs = 0;
-      for (int64_t k = sg.x + gl; k < sg.y; k += 8) cs += t.hit(__ldg(radj + k));
-      c += cs;
-      sg = nx;
-    }
-  }
-#endif
   return c;
 }
 
