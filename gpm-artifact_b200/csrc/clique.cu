@@ -175,9 +175,75 @@ __device__ __forceinline__ WarpSet wrow(const uint32_t *rows, int W, int j, unsi
   return s;
 }
 
+// index of the k-th (0-based) set bit of w (k < popc(w))
+__device__ __forceinline__ int kth_bit(uint32_t w, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int s = 16; s; s >>= 1) {
+    const int c = __popc(w & ((1u << s) - 1u));
+    if (k >= c) {
+      k -= c;
+      w >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
+
+// Sum over l in X of |X & row_l| -- the 2-cliques inside warp-spread X --
+// with the members l of X spread over the lanes: lane t takes the t-th
+// member of each round of 32 and ANDs X (staged in the warp's shared words
+// xs) with its row word by word from l's own word on (row_l has no bits
+// below l).  Each lane returns its partial sum.
+__device__ unsigned long long wsum_pairs(const uint32_t *rows, int W, WarpSet X, uint32_t *xs, unsigned lane) {
+  __syncwarp();
+  xs[lane] = X.a;
+  xs[lane + 32] = X.b;
+  __syncwarp();
+  // members are numbered word by word: words 0..31 (X.a of lanes 0..31), then 32..63
+  int inc = __popc(X.a), incb = __popc(X.b);
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int va = __shfl_up_sync(0xffffffffu, inc, o), vb = __shfl_up_sync(0xffffffffu, incb, o);
+    if ((int)lane >= o) {
+      inc += va;
+      incb += vb;
+    }
+  }
+  const int ta = __shfl_sync(0xffffffffu, inc, 31), total = ta + __shfl_sync(0xffffffffu, incb, 31);
+  unsigned long long c = 0;
+  for (int base = 0; base < total; base += 32) {
+    const int idx = base + (int)lane;
+    // word holding member idx: first word whose inclusive prefix exceeds it
+    const bool hi = idx >= ta;
+    const int key = hi ? idx - ta : idx;
+    int lo = 0, up = 31;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const int mid = (lo + up) >> 1;
+      const int pa = __shfl_sync(0xffffffffu, inc, mid), pb = __shfl_sync(0xffffffffu, incb, mid);
+      if ((hi ? pb : pa) > key) up = mid; else lo = mid + 1;
+    }
+    const int pa_lo = __shfl_sync(0xffffffffu, inc, lo), pb_lo = __shfl_sync(0xffffffffu, incb, lo);
+    if (idx < total) {
+      const int w = lo + (hi ? 32 : 0);
+      const uint32_t word = xs[w];
+      const int excl = (hi ? pb_lo : pa_lo) - __popc(word);
+      const int l = w * 32 + kth_bit(word, key - excl);
+      const uint32_t *rl = rows + (size_t)l * W;
+      unsigned s = 0;
+      for (int ww = l >> 5; ww < W; ++ww) s += __popc(xs[ww] & rl[ww]);
+      c += s;
+    }
+  }
+  return c;
+}
+
 // q-cliques inside warp-spread X; stk holds (q) levels of W words per warp
-__device__ unsigned long long warp_count_set(const uint32_t *rows, int W, WarpSet X, int q, unsigned lane) {
+__device__ unsigned long long warp_count_set(const uint32_t *rows, int W, WarpSet X, int q, uint32_t *xs,
+                                             unsigned lane) {
   if (q == 1) return (unsigned long long)wpop(X);
+  if (q == 2) return wsum_pairs(rows, W, X, xs, lane);
   WarpSet stk[kCqMaxK];
   int depth = 0;
   stk[0] = X;
@@ -189,13 +255,15 @@ __device__ unsigned long long warp_count_set(const uint32_t *rows, int W, WarpSe
     WarpSet Y{stk[depth].a & r.a, stk[depth].b & r.b};
     int left = q - depth - 1;
     if (left == 1) c += (unsigned long long)wpop(Y);
+    else if (left == 2) c += wsum_pairs(rows, W, Y, xs, lane);
     else stk[++depth] = Y;
   }
   return c;
 }
 
 __device__ unsigned long long clique_cta_task(int32_t u, int k, const int64_t *__restrict__ roff,
-                                              const int32_t *__restrict__ radj, char *smem, uint32_t *slab) {
+                                              const int32_t *__restrict__ radj, char *smem, uint32_t *slab,
+                                              uint32_t *xs) {
   const int tid = threadIdx.x, nthr = blockDim.x, wid = tid >> 5, nw = nthr >> 5;
   const unsigned lane = tid & 31;
   const int64_t s0 = roff[u];
@@ -224,7 +292,7 @@ __device__ unsigned long long clique_cta_task(int32_t u, int k, const int64_t *_
   __syncthreads();
   unsigned long long c = 0;
   // each lane accumulates the popcounts of its own words; the warp sum is the count
-  for (int i = wid; i < d; i += nw) c += warp_count_set(rows, W, wrow(rows, W, i, lane), k - 2, lane);
+  for (int i = wid; i < d; i += nw) c += warp_count_set(rows, W, wrow(rows, W, i, lane), k - 2, xs, lane);
   __syncthreads();
   return c;
 }
@@ -238,6 +306,7 @@ __global__ void __launch_bounds__(256) k_clique_local(int k, const int64_t *__re
                                                       unsigned long long *__restrict__ acc, int stride, int slot) {
   extern __shared__ __align__(16) char csm[];
   __shared__ int s_task;
+  __shared__ uint32_t sxs[8][64];  // each warp's staged set (wsum_pairs)
   const int wid = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31;
   uint32_t *slab = slabs + (size_t)blockIdx.x * slab_words;
@@ -248,7 +317,7 @@ __global__ void __launch_bounds__(256) k_clique_local(int k, const int64_t *__re
     __syncthreads();
     if (t >= n_cta) break;
     const int32_t u = cta_tasks[t];
-    unsigned long long c = warp_sum(clique_cta_task(u, k, roff, radj, csm, slab));
+    unsigned long long c = warp_sum(clique_cta_task(u, k, roff, radj, csm, slab, sxs[wid]));
     if (lane == 0 && c) atomicAdd(&acc[(size_t)stride * (gid ? gid[u] : 0) + slot], c);
   }
   int32_t *L = reinterpret_cast<int32_t *>(csm + wid * (kCqWarpMax * 12));
