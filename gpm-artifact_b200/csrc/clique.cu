@@ -118,16 +118,51 @@ __device__ unsigned long long clique_warp_task(int32_t u, int k, const int64_t *
   }
   __syncwarp();
   const int32_t kmax = L[d - 1];
-  // row i: members of L inside N+(L[i]) (all > L[i]); scan up to kmax only
-  for (int i = 0; i < d; ++i) {
-    int32_t v = L[i];
-    int64_t s = roff[v], e = roff[v + 1];
-    int64_t stop = s;
-    if (lane == 0) stop = s + upper_bound_g(radj + s, e - s, kmax);
-    stop = __shfl_sync(0xffffffffu, stop, 0);
-    for (int64_t t = s + lane; t < stop; t += 32) {
-      int p = find_pos(L, d, __ldg(radj + t));
-      if (p >= 0) atomicOr(&rows[i], 1ull << p);
+  // row i: members of L inside N+(L[i]) (all > L[i]); only N+(L[i]) up to
+  // kmax can hit.  Lane j finds the scan ranges of rows j and j + 32 (one
+  // binary search each, in parallel), then the ranges are laid end to end
+  // and every lane takes one entry of the concatenation per round, so short
+  // lists do not leave lanes idle.
+  long long sa = 0, la = 0, sb = 0, lb = 0;
+  if ((int)lane < d) {
+    const int32_t v = L[lane];
+    sa = roff[v];
+    la = upper_bound_g(radj + sa, roff[v + 1] - sa, kmax);
+  }
+  if ((int)lane + 32 < d) {
+    const int32_t v = L[lane + 32];
+    sb = roff[v];
+    lb = upper_bound_g(radj + sb, roff[v + 1] - sb, kmax);
+  }
+  long long ia = la, ib = lb;  // inclusive prefixes over rows 0..31 and 32..63
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long va = __shfl_up_sync(0xffffffffu, ia, o), vb = __shfl_up_sync(0xffffffffu, ib, o);
+    if ((int)lane >= o) {
+      ia += va;
+      ib += vb;
+    }
+  }
+  const long long ta = __shfl_sync(0xffffffffu, ia, 31), total = ta + __shfl_sync(0xffffffffu, ib, 31);
+  for (long long base = 0; base < total; base += 32) {
+    const long long idx = base + lane;
+    const bool hi = idx >= ta;
+    const long long key = hi ? idx - ta : idx;
+    int lo = 0, up = 31;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      const int mid = (lo + up) >> 1;
+      const long long pa = __shfl_sync(0xffffffffu, ia, mid), pb = __shfl_sync(0xffffffffu, ib, mid);
+      if ((hi ? pb : pa) > key) up = mid; else lo = mid + 1;
+    }
+    const long long pa = __shfl_sync(0xffffffffu, ia, lo), pb = __shfl_sync(0xffffffffu, ib, lo);
+    const long long ra = __shfl_sync(0xffffffffu, la, lo), rb = __shfl_sync(0xffffffffu, lb, lo);
+    const long long xa = __shfl_sync(0xffffffffu, sa, lo), xb = __shfl_sync(0xffffffffu, sb, lo);
+    if (idx < total) {
+      const int row = lo + (hi ? 32 : 0);
+      const long long t = (hi ? xb : xa) + key - ((hi ? pb : pa) - (hi ? rb : ra));
+      const int p = find_pos(L, d, __ldg(radj + t));
+      if (p >= 0) atomicOr(&rows[row], 1ull << p);
     }
   }
   __syncwarp();
@@ -277,16 +312,24 @@ __device__ unsigned long long clique_cta_task(int32_t u, int k, const int64_t *_
   for (size_t i = tid; i < (size_t)d * W; i += nthr) rows[i] = 0u;
   __syncthreads();
   const int32_t kmax = L[d - 1];
-  for (int i = wid; i < d; i += nw) {
-    int32_t v = L[i];
-    int64_t s = roff[v], e = roff[v + 1];
-    int64_t stop = s;
-    if (lane == 0) stop = s + upper_bound_g(radj + s, e - s, kmax);
-    stop = __shfl_sync(0xffffffffu, stop, 0);
-    uint32_t *ri = rows + (size_t)i * W;
-    for (int64_t t = s + lane; t < stop; t += 32) {
-      int p = find_pos(L, d, __ldg(radj + t));
-      if (p >= 0) atomicOr(&ri[p >> 5], 1u << (p & 31));
+  // warp wid builds rows wid, wid + nw, ...; the scan ranges of 32 of them at
+  // a time are found in parallel, one lane per row
+  for (int i0 = wid; i0 < d; i0 += nw * 32) {
+    const int mine = i0 + (int)lane * nw;
+    long long ms = 0, mstop = 0;
+    if (mine < d) {
+      const int32_t v = L[mine];
+      ms = roff[v];
+      mstop = ms + upper_bound_g(radj + ms, roff[v + 1] - ms, kmax);
+    }
+    for (int j = 0; j < 32 && i0 + j * nw < d; ++j) {
+      const int i = i0 + j * nw;
+      const long long s = __shfl_sync(0xffffffffu, ms, j), stop = __shfl_sync(0xffffffffu, mstop, j);
+      uint32_t *ri = rows + (size_t)i * W;
+      for (long long t = s + lane; t < stop; t += 32) {
+        int p = find_pos(L, d, __ldg(radj + t));
+        if (p >= 0) atomicOr(&ri[p >> 5], 1u << (p & 31));
+      }
     }
   }
   __syncthreads();
