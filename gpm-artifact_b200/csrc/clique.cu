@@ -484,14 +484,13 @@ __global__ void __launch_bounds__(256) k_clique_edge(int64_t nnz, int k, const i
 
 // ------------------------------------------------------------ host
 static int clique_local_grid() {
-  static int grid = 0;
-  if (!grid) {
+  static PerDevice grid;
+  return grid.get([] {
     cudaFuncSetAttribute(k_clique_local, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCqSmem);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clique_local, 256, kCqSmem);
-    grid = std::max(1, per_sm) * num_sms();
-  }
-  return grid;
+    return std::max(1, per_sm) * num_sms();
+  });
 }
 
 // Plan: task queues (heaviest first) and row slabs; the run is launches only.

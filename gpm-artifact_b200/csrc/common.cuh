@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 
 #include "gpm.h"
@@ -239,4 +240,25 @@ void free_clique_plan(CliquePlan *p);  // clique.cu
 // Drops every cached schedule (after the stored graph changed).
 void drop_plans(gpm_graph *g);
 int num_sms();
+
+// A launch parameter (a persistent grid size, after the kernel's attributes
+// are set) computed by `init` the first time it is needed on each device,
+// with that device current: function attributes and SM counts are per
+// device.
+struct PerDevice {
+  static constexpr int kDevices = 64;
+  std::atomic<int> v[kDevices] = {};
+  template <class F>
+  int get(F init) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kDevices) return init();
+    int x = v[dev].load(std::memory_order_relaxed);
+    if (!x) {
+      x = init();
+      v[dev].store(x, std::memory_order_relaxed);
+    }
+    return x;
+  }
+};
 }  // namespace gpm

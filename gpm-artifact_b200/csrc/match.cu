@@ -731,12 +731,12 @@ static int match_run(gpm_graph *g, const gpm_query *q, unsigned long long limit,
     GPM_LAUNCH_CHECK();
     return finish(np);
   }
-  static int per_sm = 0;
-  if (!per_sm) {
+  static PerDevice match_grid;
+  const int grid = match_grid.get([] {
+    int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match<false>, kMatchWarps * 32, 0);
-    per_sm = std::max(1, per_sm);
-  }
-  const int grid = per_sm * num_sms();
+    return std::max(1, per_sm) * num_sms();
+  });
   const HubIndex hub{lc->hub_slot.p, lc->hub_bm.p, lc->hub_words};
   DevBuf<unsigned long long> cursor;
   GPM_TRY(cursor.reserve(1));
@@ -943,13 +943,12 @@ static int batch_tasks(gpm_match_batch *b, int64_t span) {
 }
 
 static int batch_grid() {
-  static int grid = 0;
-  if (!grid) {
+  static PerDevice grid;
+  return grid.get([] {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_batch, kMatchWarps * 32, 0);
-    grid = std::max(1, per_sm) * num_sms();
-  }
-  return grid;
+    return std::max(1, per_sm) * num_sms();
+  });
 }
 
 static int batch_launch(gpm_match_batch *b, cudaStream_t st) {

@@ -680,13 +680,12 @@ static int dag_from_split(int64_t n, const int64_t *roff, const int64_t *split, 
 }
 
 static int te_grid() {
-  static int grid = 0;
-  if (!grid) {
+  static PerDevice grid;
+  return grid.get([] {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_edge_tri, 256, kTeSmem);
-    grid = std::max(1, per_sm) * num_sms();
-  }
-  return grid;
+    return std::max(1, per_sm) * num_sms();
+  });
 }
 
 // Builds every schedule and scratch buffer of the pipeline (host syncs and

@@ -322,15 +322,13 @@ __global__ void k_tc_split(int64_t n, const int64_t *__restrict__ off, int warp_
 void free_tc_plan(TcPlan *p) { delete p; }
 
 int tc_hash_grid() {
-  static int grid = 0;
-  if (!grid) {
+  static PerDevice grid;
+  return grid.get([] {
     int per_sm = 0;
     cudaFuncSetAttribute(k_tc_hash, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_hash, 256, TC_SMEM);
-    if (per_sm < 1) per_sm = 1;
-    grid = per_sm * num_sms();
-  }
-  return grid;
+    return std::max(1, per_sm) * num_sms();
+  });
 }
 
 int tc_build_plan(gpm_graph *g, int warp_min, int cta_min, cudaStream_t st) {

@@ -893,13 +893,12 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
 }
 
 static int rank_grid() {
-  static int grid = 0;
-  if (!grid) {
+  static PerDevice grid;
+  return grid.get([] {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_rank, 256, kRankSmem);
-    grid = std::max(1, per_sm) * num_sms();
-  }
-  return grid;
+    return std::max(1, per_sm) * num_sms();
+  });
 }
 
 // Launch of a given plan; rec != nullptr selects the instrumented build.
