@@ -663,7 +663,7 @@ def match_workload(args, stream):
         k, e, ql = queries[name]
         q = gpm.Query(k, e[:, 0], e[:, 1], ql)
         first, c = event_ms(lambda: g.match(q), stream)
-        reps = 1 if first[0] > 2000 else max(1, min(args.steps, 5))
+        reps = 2 if first[0] > 2000 else max(1, min(args.steps, 5))
         ms, c2 = event_ms(lambda: g.match(q), stream, reps)
         assert c2 == c
         avg = sum(ms) / len(ms)

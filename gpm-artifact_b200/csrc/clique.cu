@@ -33,10 +33,12 @@ constexpr int kCqWarpMax = 64;      // warp tasks: |L| <= 64
 constexpr int kCqCtaMax = 2048;     // CTA tasks: |L| <= 2048 (W <= 64)
 constexpr int kCqMaxK = 8;
 #ifndef GPM_CQ_SMEM_KB
-// 48 KB: 4 CTAs per SM.  R-MAT 20, median of 3: 4-cliques 55 ms, 5-cliques
-// 1.15 s, against 89 ms / 1.71 s at 96 KB (2 CTAs per SM, a quarter of the
-// warp slots); tasks whose rows do not fit use their CTA's global slab
-#define GPM_CQ_SMEM_KB 48
+// 32 KB: 5 CTAs per SM (registers allow 5; 48 KB allowed 4).  R-MAT 20 with
+// the lane-parallel last levels: 4-cliques 24.1 ms, 5-cliques 188 ms against
+// 27.0 / 194 ms at 48 KB and 24.3 / 195 ms at 40 KB (motif batch replay 809
+// against 835 ms).  Earlier, 48 KB beat 96 KB (2 CTAs per SM) by 1.6x.
+// Tasks whose rows do not fit use their CTA's global slab.
+#define GPM_CQ_SMEM_KB 32
 #endif
 constexpr size_t kCqSmem = GPM_CQ_SMEM_KB * 1024;  // dynamic shared memory per CTA
 
