@@ -135,7 +135,8 @@ struct MatchGraph {
 // returns the count (TRACK: counted into *found instead, see k_match).
 // chunk >= 0 restricts position 2's candidates to the `span` entries from
 // `chunk` on (tasks split by the batch path); buf is the warp's shared
-// buffer of kMaxQ - 2 rows of 32 candidates.
+// buffer of kMaxQ rows of 32 candidates (rows d - 2 for positions 2 .. n-2,
+// the last two for the pool of position n-2's survivors).
 template <bool TRACK>
 __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, const MatchGraph &G, int32_t root,
                                                          int32_t second, int64_t chunk, int64_t span,
@@ -202,16 +203,18 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
     return __popc(m);
   };
 
-  // embeddings completing positions 0 .. n-3 with y = ys (lane t < k holds
-  // candidate t of position n-2) and some last vertex
-  auto close = [&](int32_t y, int k) {
+  // embeddings completing positions 0 .. n-4 with (z, y) at positions
+  // (n-3, n-2) (lane t < k holds pair t: pairs from several parents z are
+  // pooled) and some last vertex
+  auto close = [&](int32_t z, int32_t y, int k) {
+    const int par = pre - 1;
     // lane t: its candidate's shortest segment for the last vertex
     int src = -1;
     long long st = 0, len = 0;
     if ((int)lane < k) {
       for (uint32_t bm = lmask; bm; bm &= bm - 1) {
         const int j = __ffs(bm) - 1;
-        const int32_t a = j == pre ? y : emb[j];
+        const int32_t a = j == pre ? y : j == par ? z : emb[j];
         int64_t s, e;
         seg_range(off, loff, L, a, llab, &s, &e);
         if (src < 0 || e - s < len) {
@@ -242,16 +245,16 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
       const long long pt = __shfl_sync(0xffffffffu, inc, t), lt = __shfl_sync(0xffffffffu, len, t);
       const long long stt = __shfl_sync(0xffffffffu, st, t);
       const int srct = __shfl_sync(0xffffffffu, src, t);
-      const int32_t yt = __shfl_sync(0xffffffffu, y, t);
+      const int32_t yt = __shfl_sync(0xffffffffu, y, t), zt = __shfl_sync(0xffffffffu, z, t);
       bool ok = false;
       int32_t x = 0;
       if (idx < total) {
         x = __ldg(ladj + stt + (idx - (pt - lt)));
-        ok = (L > 0 || labels[x] == llab) && x != yt;
-        for (int j = 0; ok && j < pre; ++j) ok = emb[j] != x;
+        ok = (L > 0 || labels[x] == llab) && x != yt && x != zt;
+        for (int j = 0; ok && j < par; ++j) ok = emb[j] != x;
         for (uint32_t bm = lmask & ~(1u << srct); ok && bm; bm &= bm - 1) {
           const int j = __ffs(bm) - 1;
-          ok = adjacent(hub, off, adj, ladj, loff, L, j == pre ? yt : emb[j], llab, x);
+          ok = adjacent(hub, off, adj, ladj, loff, L, j == pre ? yt : j == par ? zt : emb[j], llab, x);
         }
       }
       const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -262,7 +265,8 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
         const unsigned long long slot = at + __popc(m & ((1u << lane) - 1u));
         if (emb_out && ok && slot < limit) {
           int32_t *row = emb_out + slot * (unsigned long long)q.n;
-          for (int j = 0; j < pre; ++j) row[q.order[j]] = emb[j];
+          for (int j = 0; j < par; ++j) row[q.order[j]] = emb[j];
+          row[q.order[par]] = zt;
           row[q.order[pre]] = yt;
           row[q.order[last]] = x;
         }
@@ -274,9 +278,16 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
   emb[0] = root;
   emb[1] = second;
   if (pre == 1) {  // three query vertices: the pair's second vertex is position n-2
-    close(second, 1);
+    close(root, second, 1);
     return c;
   }
+  // survivors of position n-2 pooled with their parent at n-3 (rows
+  // kMaxQ-2 / kMaxQ-1 of buf) until 32 are pending or position n-4 moves on
+  int np = 0;
+  auto flush = [&]() {
+    if (np) close((int)lane < np ? buf[kMaxQ - 1][lane] : 0, (int)lane < np ? buf[kMaxQ - 2][lane] : 0, np);
+    np = 0;
+  };
   int d = 2;
   open(2);
   if (chunk >= 0) {
@@ -292,7 +303,15 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
         continue;
       }
       const int k = fill(d);
-      if (k) close((int)lane < k ? buf[d - 2][lane] : 0, k);
+      if (k) {
+        if (np + k > 32) flush();
+        if ((int)lane < k) {
+          buf[kMaxQ - 2][np + lane] = buf[d - 2][lane];
+          buf[kMaxQ - 1][np + lane] = emb[pre - 1];
+        }
+        __syncwarp();
+        np += k;
+      }
       continue;
     }
     if (bcur[d] < bcnt[d]) {
@@ -307,8 +326,10 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
       bcur[d] = 0;
       continue;
     }
+    if (d == pre - 1) flush();  // position n-4 is about to move on
     --d;
   }
+  flush();
   return c;
 }
 
@@ -318,12 +339,18 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
 // data-vertex ids per embedding, in query-vertex order), and the whole grid
 // stops once `limit` are found (sub_ceci's -num, myceci.cpp:615-617).
 // Otherwise the count goes to *out.
+#ifndef GPM_MATCH_MIN_BLOCKS
+// 6 CTAs per SM (at most 40 registers): R-MAT 21 4-cycle 1.81 s, diamond
+// 3.78-3.83 s, R-MAT 18 house 5.25 s against 2.23-2.49 / 4.05 / 5.5 s at the
+// 48 registers the compiler picks unbounded (5 CTAs per SM)
+#define GPM_MATCH_MIN_BLOCKS 6
+#endif
 template <bool TRACK>
-__global__ void __launch_bounds__(kMatchWarps * 32)
+__global__ void __launch_bounds__(kMatchWarps * 32, GPM_MATCH_MIN_BLOCKS)
     k_match(QueryPlan q, MatchGraph G, const int2 *__restrict__ pairs, int64_t n,
             unsigned long long *__restrict__ cursor, unsigned long long *__restrict__ out, unsigned long long limit,
             unsigned long long *found, int32_t *__restrict__ emb_out) {
-  __shared__ int32_t sbuf[kMatchWarps][kMaxQ - 2][32];
+  __shared__ int32_t sbuf[kMatchWarps][kMaxQ][32];
   const unsigned lane = lane_id();
   unsigned long long c = 0;
   while (true) {
@@ -814,7 +841,7 @@ __global__ void __launch_bounds__(kMatchWarps * 32)
     k_match_batch(const QueryPlan *__restrict__ plans, MatchGraph G, const int4 *__restrict__ tasks, int64_t ntasks,
                   int64_t span, const int32_t *__restrict__ member, int nm, unsigned long long *__restrict__ cursor,
                   unsigned long long *__restrict__ out) {
-  __shared__ int32_t sbuf[kMatchWarps][kMaxQ - 2][32];
+  __shared__ int32_t sbuf[kMatchWarps][kMaxQ][32];
   __shared__ QueryPlan splan[kMatchWarps];
   static_assert(sizeof(QueryPlan) % 4 == 0, "plan copied as words");
   const int w = threadIdx.x >> 5;
