@@ -97,8 +97,8 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
                                                             int64_t l1, int64_t s0, int64_t s1, const T &t,
                                                             int wid, int nw, unsigned lane) {
   unsigned long long c = 0;
-  const unsigned half = lane >> 4, hl = lane & 15;
   int64_t j;
+  const unsigned half = lane >> 4, hl = lane & 15;
   for (j = l0 + wid * 2 + half; j < l1; j += nw * 2) {
     const longlong2 sg = pseg[j];
     const int32_t *__restrict__ q = radj + sg.x;

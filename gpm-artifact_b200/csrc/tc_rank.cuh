@@ -23,7 +23,10 @@ constexpr int kRankCtaMin = GPM_RANK_CTA_MIN;
 // fixed schedule: partner segments of at least this many keys are streamed
 // by a half-warp, shorter ones by 8-lane groups (R-MAT 20: 1.35 ms at 64,
 // 1.38 ms at 32)
-constexpr int kRankLongMin = 64;
+#ifndef GPM_RANK_LONG_MIN
+#define GPM_RANK_LONG_MIN 64
+#endif
+constexpr int kRankLongMin = GPM_RANK_LONG_MIN;
 
 // The stored graph renumbered by (in + out degree, id) rank, lists sorted.
 // upward == 1 when every stored edge points to a larger rank, which holds
