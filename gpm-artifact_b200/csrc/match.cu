@@ -6,43 +6,74 @@
 // are separate embeddings).  Its CECI filter and tree only prune; the count
 // is that number.
 //
-// GPU design: the query (<= 16 vertices) is ordered on the host -- start at
+// GPU design: the query (<= 64 vertices, sub_ceci's MAX_QUERY_VERTEX in
+// sub_ceci/configuration/config.h:12) is ordered on the host -- start at
 // the vertex whose label is rarest in the data graph (ties: higher degree),
 // then repeatedly the unplaced vertex with most placed neighbours.  The data
 // graph's lists are partitioned by label, so the candidates of a query
 // vertex are one label segment of a mapped neighbour's list (the shortest
 // one), and the other back-edges are checked by one bit test (vertices with
 // an adjacency bitmap) or a binary search inside a label segment.  Tasks are
-// the (root, second vertex) pairs, drained from an atomic cursor by a
-// persistent grid; each warp walks its task depth first (k_match).
+// the (root, second vertex) pairs -- extended breadth first to longer
+// partial embeddings while they are too few to fill the GPU -- drained from
+// an atomic cursor by a persistent grid; each warp walks its task depth first
+// (k_match).
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
 
-constexpr int kMaxQ = 16;
+constexpr int kMaxQ = 64;     // query vertices (sub_ceci/configuration/config.h:12)
+constexpr int kNarrowQ = 16;  // plans up to this size take the narrow kernels
 
 struct gpm_query {
   int n = 0;
   int32_t labels[kMaxQ];
-  uint32_t adjmask[kMaxQ];  // bit j set iff query edge (i, j)
+  unsigned long long adjmask[kMaxQ];  // bit j set iff query edge (i, j)
   int deg[kMaxQ];
 };
 
 namespace gpm {
 
-struct QueryPlan {
+// A query in matching order, for queries of at most Q vertices.  Q = 16:
+// 32-bit position masks and the kernels' static shared buffers (the common
+// case, 6 CTAs per SM); Q = 64: 64-bit masks and buffers in dynamic shared
+// memory.
+template <int Q>
+struct QueryPlanT {
+  using Mask = typename std::conditional<(Q <= 32), uint32_t, unsigned long long>::type;
   int n;
-  int order[kMaxQ];
-  int parent_pos[kMaxQ];      // position (in order) of the parent, -1 for the root
-  uint32_t back_pos[kMaxQ];   // bitmask of earlier positions that must be adjacent (parent excluded)
-  int32_t label[kMaxQ];       // label of the vertex at each position
-  int mindeg[kMaxQ];          // query degree at each position
+  int order[Q];
+  int parent_pos[Q];  // position (in order) of the parent, -1 for the root
+  Mask back_pos[Q];   // bitmask of earlier positions that must be adjacent (parent excluded)
+  int32_t label[Q];   // label of the vertex at each position
+  int mindeg[Q];      // query degree at each position
 };
+using QueryPlan = QueryPlanT<kNarrowQ>;
+using WidePlan = QueryPlanT<kMaxQ>;
+
+// The plan of a query of at most Q vertices in the Q-wide layout.
+template <int Q>
+static void narrow_plan(const WidePlan &w, QueryPlanT<Q> *p) {
+  memset(p, 0, sizeof *p);
+  p->n = w.n;
+  for (int k = 0; k < w.n && k < Q; ++k) {
+    p->order[k] = w.order[k];
+    p->parent_pos[k] = w.parent_pos[k];
+    p->back_pos[k] = (typename QueryPlanT<Q>::Mask)w.back_pos[k];
+    p->label[k] = w.label[k];
+    p->mindeg[k] = w.mindeg[k];
+  }
+}
+
+// Index of the lowest set bit of a non-zero position mask.
+__device__ __forceinline__ int low_bit(uint32_t m) { return __ffs(m) - 1; }
+__device__ __forceinline__ int low_bit(unsigned long long m) { return __ffsll((long long)m) - 1; }
 
 __device__ __forceinline__ bool has_edge(const int64_t *__restrict__ off, const int32_t *__restrict__ adj, int32_t a,
                                          int32_t key) {
@@ -131,15 +162,18 @@ struct MatchGraph {
   HubIndex hub;
 };
 
-// The embeddings of one (root, second vertex) task, by one warp; lane 0
-// returns the count (TRACK: counted into *found instead, see k_match).
-// chunk >= 0 restricts position 2's candidates to the `span` entries from
-// `chunk` on (tasks split by the batch path); buf is the warp's shared
-// buffer of kMaxQ rows of 32 candidates (rows d - 2 for positions 2 .. n-2,
+// The embeddings extending one partial embedding `row` (positions 0 .. t-1
+// mapped, t >= 2: a (root, second vertex) pair, or a row of a breadth-first
+// extension), by one warp; lane 0 returns the count (TRACK: counted into
+// *found instead, see k_match).  chunk >= 0 restricts position t's
+// candidates to the `span` entries from `chunk` on (tasks split by the batch
+// path); buf is the warp's shared
+// buffer of Q rows of 32 candidates (rows d - 2 for positions 2 .. n-2,
 // the last two for the pool of position n-2's survivors).
-template <bool TRACK>
-__device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, const MatchGraph &G, int32_t root,
-                                                         int32_t second, int64_t chunk, int64_t span,
+template <bool TRACK, int Q>
+__device__ __forceinline__ unsigned long long match_task(const QueryPlanT<Q> &q, const MatchGraph &G,
+                                                         const int32_t *__restrict__ row, int t, int64_t chunk,
+                                                         int64_t span,
                                                          int32_t (*buf)[32], unsigned long long limit,
                                                          unsigned long long *found, int32_t *__restrict__ emb_out) {
   const int64_t *__restrict__ off = G.off;
@@ -149,27 +183,28 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
   const int32_t *__restrict__ labels = G.labels;
   const int L = G.L;
   const HubIndex &hub = G.hub;
+  using Mask = typename QueryPlanT<Q>::Mask;
   const unsigned lane = lane_id();
-  int32_t emb[kMaxQ] = {};
-  int64_t pos[kMaxQ], end[kMaxQ];
-  uint32_t chk[kMaxQ];
-  int bcnt[kMaxQ], bcur[kMaxQ];
+  int32_t emb[Q] = {};
+  int64_t pos[Q], end[Q];
+  Mask chk[Q];
+  int bcnt[Q], bcur[Q];
   const int last = q.n - 1, pre = q.n - 2;
   const int llab = q.label[last];
-  const uint32_t lmask = q.back_pos[last] | (1u << q.parent_pos[last]);
+  const Mask lmask = q.back_pos[last] | ((Mask)1 << q.parent_pos[last]);
   unsigned long long c = 0;
 
   // candidate segment of position d: the shortest label segment among the
   // mapped query-neighbours, the others left to check (chk)
   auto open = [&](int d) {
     const int lab = q.label[d];
-    uint32_t nb = q.back_pos[d] | (1u << q.parent_pos[d]);
+    const Mask nb = q.back_pos[d] | ((Mask)1 << q.parent_pos[d]);
     int src = q.parent_pos[d];
     int64_t s, e;
     seg_range(off, loff, L, emb[src], lab, &s, &e);
     if (L > 0)
-      for (uint32_t bm = q.back_pos[d]; bm; bm &= bm - 1) {
-        const int j = __ffs(bm) - 1;
+      for (Mask bm = q.back_pos[d]; bm; bm &= bm - 1) {
+        const int j = low_bit(bm);
         int64_t sj, ej;
         seg_range(off, loff, L, emb[j], lab, &sj, &ej);
         if (ej - sj < e - s) {
@@ -178,7 +213,7 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
           e = ej;
         }
       }
-    chk[d] = nb & ~(1u << src);
+    chk[d] = nb & ~((Mask)1 << src);
     pos[d] = off[emb[src]] + s;
     end[d] = off[emb[src]] + e;
   };
@@ -193,8 +228,8 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
       x = __ldg(ladj + i);
       ok = (L > 0 || labels[x] == lab) && off[x + 1] - off[x] >= q.mindeg[d];
       for (int j = 0; ok && j < d; ++j) ok = emb[j] != x;
-      for (uint32_t bm = chk[d]; ok && bm; bm &= bm - 1)
-        ok = adjacent(hub, off, adj, ladj, loff, L, emb[__ffs(bm) - 1], lab, x);
+      for (Mask bm = chk[d]; ok && bm; bm &= bm - 1)
+        ok = adjacent(hub, off, adj, ladj, loff, L, emb[low_bit(bm)], lab, x);
     }
     pos[d] += 32;
     const unsigned m = __ballot_sync(0xffffffffu, ok);
@@ -212,8 +247,8 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
     int src = -1;
     long long st = 0, len = 0;
     if ((int)lane < k) {
-      for (uint32_t bm = lmask; bm; bm &= bm - 1) {
-        const int j = __ffs(bm) - 1;
+      for (Mask bm = lmask; bm; bm &= bm - 1) {
+        const int j = low_bit(bm);
         const int32_t a = j == pre ? y : j == par ? z : emb[j];
         int64_t s, e;
         seg_range(off, loff, L, a, llab, &s, &e);
@@ -252,8 +287,8 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
         x = __ldg(ladj + stt + (idx - (pt - lt)));
         ok = (L > 0 || labels[x] == llab) && x != yt && x != zt;
         for (int j = 0; ok && j < par; ++j) ok = emb[j] != x;
-        for (uint32_t bm = lmask & ~(1u << srct); ok && bm; bm &= bm - 1) {
-          const int j = __ffs(bm) - 1;
+        for (Mask bm = lmask & ~((Mask)1 << srct); ok && bm; bm &= bm - 1) {
+          const int j = low_bit(bm);
           ok = adjacent(hub, off, adj, ladj, loff, L, j == pre ? yt : j == par ? zt : emb[j], llab, x);
         }
       }
@@ -275,27 +310,26 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
     }
   };
 
-  emb[0] = root;
-  emb[1] = second;
-  if (pre == 1) {  // three query vertices: the pair's second vertex is position n-2
-    close(root, second, 1);
+  for (int j = 0; j < t; ++j) emb[j] = row[j];
+  if (pre == t - 1) {  // the row already maps position n-2
+    close(emb[pre - 1], emb[pre], 1);
     return c;
   }
   // survivors of position n-2 pooled with their parent at n-3 (rows
-  // kMaxQ-2 / kMaxQ-1 of buf) until 32 are pending or position n-4 moves on
+  // Q-2 / Q-1 of buf) until 32 are pending or position n-4 moves on
   int np = 0;
   auto flush = [&]() {
-    if (np) close((int)lane < np ? buf[kMaxQ - 1][lane] : 0, (int)lane < np ? buf[kMaxQ - 2][lane] : 0, np);
+    if (np) close((int)lane < np ? buf[Q - 1][lane] : 0, (int)lane < np ? buf[Q - 2][lane] : 0, np);
     np = 0;
   };
-  int d = 2;
-  open(2);
+  int d = t;
+  open(t);
   if (chunk >= 0) {
-    pos[2] += chunk;
-    end[2] = min(end[2], pos[2] + span);
+    pos[t] += chunk;
+    end[t] = min(end[t], pos[t] + span);
   }
-  bcnt[2] = bcur[2] = 0;
-  while (d >= 2) {
+  bcnt[t] = bcur[t] = 0;
+  while (d >= t) {
     if (TRACK && *(volatile unsigned long long *)found >= limit) break;
     if (d == pre) {
       if (pos[d] >= end[d]) {
@@ -306,8 +340,8 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
       if (k) {
         if (np + k > 32) flush();
         if ((int)lane < k) {
-          buf[kMaxQ - 2][np + lane] = buf[d - 2][lane];
-          buf[kMaxQ - 1][np + lane] = emb[pre - 1];
+          buf[Q - 2][np + lane] = buf[d - 2][lane];
+          buf[Q - 1][np + lane] = emb[pre - 1];
         }
         __syncwarp();
         np += k;
@@ -333,8 +367,9 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
   return c;
 }
 
-// One query over its (root, second vertex) pairs, drained from an atomic
-// cursor by a persistent grid.  TRACK: every embedding found takes a slot of
+// One query over its partial embeddings (rows of t ids: the (root, second
+// vertex) pairs, or the rows of a breadth-first extension), drained from an
+// atomic cursor by a persistent grid.  TRACK: every embedding found takes a slot of
 // *found; those below `limit` are written to emb_out (when given: q.n
 // data-vertex ids per embedding, in query-vertex order), and the whole grid
 // stops once `limit` are found (sub_ceci's -num, myceci.cpp:615-617).
@@ -345,12 +380,26 @@ __device__ __forceinline__ unsigned long long match_task(const QueryPlan &q, con
 // 48 registers the compiler picks unbounded (5 CTAs per SM)
 #define GPM_MATCH_MIN_BLOCKS 6
 #endif
-template <bool TRACK>
-__global__ void __launch_bounds__(kMatchWarps * 32, GPM_MATCH_MIN_BLOCKS)
-    k_match(QueryPlan q, MatchGraph G, const int2 *__restrict__ pairs, int64_t n,
+// Candidate rows of the wide kernels (Q > kNarrowQ): Q rows of 32 ids per
+// warp in dynamic shared memory (64 KB per CTA at Q = 64).
+template <int Q>
+constexpr int match_dyn_smem() {
+  return Q <= kNarrowQ ? 0 : kMatchWarps * Q * 32 * (int)sizeof(int32_t);
+}
+extern __shared__ __align__(16) int32_t match_dyn[];
+// The calling warp's Q rows of 32 candidates.
+template <int Q>
+__device__ __forceinline__ int32_t (*warp_rows(int32_t (*narrow)[32]))[32] {
+  return Q <= kNarrowQ ? narrow : reinterpret_cast<int32_t(*)[32]>(match_dyn + (threadIdx.x >> 5) * Q * 32);
+}
+
+template <bool TRACK, int Q>
+__global__ void __launch_bounds__(kMatchWarps * 32, Q <= kNarrowQ ? GPM_MATCH_MIN_BLOCKS : 2)
+    k_match(QueryPlanT<Q> q, MatchGraph G, const int32_t *__restrict__ rows, int t, int64_t n,
             unsigned long long *__restrict__ cursor, unsigned long long *__restrict__ out, unsigned long long limit,
             unsigned long long *found, int32_t *__restrict__ emb_out) {
-  __shared__ int32_t sbuf[kMatchWarps][kMaxQ][32];
+  __shared__ int32_t sbuf[kMatchWarps][Q <= kNarrowQ ? Q : 1][32];
+  int32_t(*buf)[32] = warp_rows<Q>(sbuf[threadIdx.x >> 5]);
   const unsigned lane = lane_id();
   unsigned long long c = 0;
   while (true) {
@@ -359,17 +408,77 @@ __global__ void __launch_bounds__(kMatchWarps * 32, GPM_MATCH_MIN_BLOCKS)
     r = __shfl_sync(0xffffffffu, r, 0);
     if (r >= (unsigned long long)n) break;
     if (TRACK && *(volatile unsigned long long *)found >= limit) break;
-    const int2 pr = pairs[r];
-    c += match_task<TRACK>(q, G, pr.x, pr.y, -1, 0, sbuf[threadIdx.x >> 5], limit, found, emb_out);
+    c += match_task<TRACK, Q>(q, G, rows + (int64_t)r * t, t, -1, 0, buf, limit, found, emb_out);
   }
   if (TRACK) return;
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(out, c);
 }
 
+// One position more for a list of partial embeddings (rows of t ids,
+// positions 0 .. t-1 mapped): every candidate of position t that passes
+// match_task's filters (its label segment of the mapped query-neighbour with
+// the shortest one, degree bound, injectivity, the other back-edges) makes a
+// row of t + 1 ids.  A warp per row; survivors are counted into *cnt and
+// written to out while their slot is below cap (out == nullptr: counted only).
+__global__ void k_extend_rows(WidePlan q, MatchGraph G, const int32_t *__restrict__ rows, int64_t nrows, int t,
+                              int32_t *__restrict__ out, unsigned long long cap,
+                              unsigned long long *__restrict__ cnt) {
+  const int64_t *__restrict__ off = G.off;
+  const int32_t *__restrict__ ladj = G.ladj;
+  const int32_t *__restrict__ loff = G.loff;
+  const int L = G.L;
+  const unsigned lane = lane_id();
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int lab = q.label[t];
+  for (int64_t r = warp; r < nrows; r += nw) {
+    const int32_t *row = rows + r * t;
+    int src = q.parent_pos[t];
+    int64_t s, e;
+    seg_range(off, loff, L, row[src], lab, &s, &e);
+    if (L > 0)
+      for (unsigned long long bm = q.back_pos[t]; bm; bm &= bm - 1) {
+        const int j = low_bit(bm);
+        int64_t sj, ej;
+        seg_range(off, loff, L, row[j], lab, &sj, &ej);
+        if (ej - sj < e - s) {
+          src = j;
+          s = sj;
+          e = ej;
+        }
+      }
+    const unsigned long long chk = (q.back_pos[t] | (1ull << q.parent_pos[t])) & ~(1ull << src);
+    const int64_t base = off[row[src]];
+    for (int64_t i0 = base + s; i0 < base + e; i0 += 32) {
+      const int64_t i = i0 + lane;
+      bool ok = false;
+      int32_t x = 0;
+      if (i < base + e) {
+        x = __ldg(ladj + i);
+        ok = (L > 0 || G.labels[x] == lab) && off[x + 1] - off[x] >= q.mindeg[t];
+        for (int j = 0; ok && j < t; ++j) ok = row[j] != x;
+        for (unsigned long long bm = chk; ok && bm; bm &= bm - 1)
+          ok = adjacent(G.hub, off, G.adj, ladj, loff, L, row[low_bit(bm)], lab, x);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (!m) continue;
+      unsigned long long at = 0;
+      if (lane == 0) at = atomicAdd(cnt, (unsigned long long)__popc(m));
+      at = __shfl_sync(0xffffffffu, at, 0);
+      const unsigned long long slot = at + __popc(m & ((1u << lane) - 1u));
+      if (out && ok && slot < cap) {
+        int32_t *o = out + slot * (unsigned long long)(t + 1);
+        for (int j = 0; j < t; ++j) o[j] = row[j];
+        o[t] = x;
+      }
+    }
+  }
+}
+
 // Embeddings of a one- or two-vertex query into emb_out (slots below
 // limit): roots with the query root's label, or the materialised pairs.
-__global__ void k_list_small(QueryPlan q, int64_t n, const int32_t *__restrict__ labels, const int64_t *__restrict__ off,
+__global__ void k_list_small(WidePlan q, int64_t n, const int32_t *__restrict__ labels, const int64_t *__restrict__ off,
                              const int2 *__restrict__ pairs, int64_t npairs, unsigned long long limit,
                              unsigned long long *__restrict__ found, int32_t *__restrict__ emb_out) {
   const int64_t tot = q.n == 1 ? n : npairs;
@@ -391,7 +500,7 @@ __global__ void k_list_small(QueryPlan q, int64_t n, const int32_t *__restrict__
 // (root, second) pairs: a warp per root with the query root's label; the
 // second vertex comes from the root's segment of the second query vertex's
 // label.  count_only: the query has two vertices, so the pairs are the answer.
-__global__ void k_match_pairs(QueryPlan q, int64_t n, const int64_t *__restrict__ off,
+__global__ void k_match_pairs(WidePlan q, int64_t n, const int64_t *__restrict__ off,
                               const int32_t *__restrict__ ladj, const int32_t *__restrict__ loff, int L,
                               const int32_t *__restrict__ labels, int count_only, int2 *__restrict__ pairs,
                               unsigned long long *__restrict__ npairs) {
@@ -451,8 +560,9 @@ __global__ void k_label_offsets(int64_t n, const int64_t *__restrict__ off, cons
   }
 }
 
-static int plan_query(const gpm_query *q, const std::vector<int64_t> &label_freq, QueryPlan *p) {
+static int plan_query(const gpm_query *q, const std::vector<int64_t> &label_freq, WidePlan *p) {
   const int n = q->n;
+  memset(p, 0, sizeof *p);
   p->n = n;
   bool placed[kMaxQ] = {false};
   int best = 0;
@@ -489,7 +599,7 @@ static int plan_query(const gpm_query *q, const std::vector<int64_t> &label_freq
     for (int j = 0; j < k; ++j) {
       if (!((q->adjmask[u] >> p->order[j]) & 1u)) continue;
       if (p->parent_pos[k] < 0) p->parent_pos[k] = j;
-      else p->back_pos[k] |= 1u << j;
+      else p->back_pos[k] |= 1ull << j;
     }
   }
   return GPM_OK;
@@ -656,7 +766,7 @@ int gpm_query_create(int64_t n, int64_t m, const int32_t *src, const int32_t *ds
                      gpm_query **out) {
   if (!out || !labels || n < 1 || m < 0 || (m > 0 && (!src || !dst)))
     return fail(GPM_EINVAL, "gpm_query_create: bad argument");
-  if (n > kMaxQ) return fail(GPM_EUNSUPPORTED, "query graphs are limited to 16 vertices");
+  if (n > kMaxQ) return fail(GPM_EUNSUPPORTED, "query graphs are limited to 64 vertices");
   gpm_query *q = new gpm_query();
   q->n = (int)n;
   for (int i = 0; i < n; ++i) {
@@ -670,10 +780,10 @@ int gpm_query_create(int64_t n, int64_t m, const int32_t *src, const int32_t *ds
       return fail(GPM_EINVAL, "query edge out of range");
     }
     if (a == b) continue;
-    q->adjmask[a] |= 1u << b;
-    q->adjmask[b] |= 1u << a;
+    q->adjmask[a] |= 1ull << b;
+    q->adjmask[b] |= 1ull << a;
   }
-  for (int i = 0; i < n; ++i) q->deg[i] = __builtin_popcount(q->adjmask[i]);
+  for (int i = 0; i < n; ++i) q->deg[i] = __builtin_popcountll(q->adjmask[i]);
   *out = q;
   return GPM_OK;
 }
@@ -686,6 +796,74 @@ int gpm_query_destroy(gpm_query *q) {
 }  // extern "C"
 
 namespace gpm {
+
+// One k_match launch over the (root, second vertex) pairs on a persistent
+// grid (occupancy x SMs, per device and plan width).
+template <int Q>
+static int launch_match(const QueryPlanT<Q> &plan, const MatchGraph &G, const int32_t *rows, int t, int64_t nrows,
+                        unsigned long long *cursor, unsigned long long *out, bool track, unsigned long long limit,
+                        unsigned long long *found, int32_t *emb) {
+  constexpr int smem = match_dyn_smem<Q>();
+  static PerDevice match_grid;
+  const int grid = match_grid.get([] {
+    if (smem > 0) {
+      cudaFuncSetAttribute(k_match<false, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      cudaFuncSetAttribute(k_match<true, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match<false, Q>, kMatchWarps * 32, smem);
+    return std::max(1, per_sm) * num_sms();
+  });
+  if (track)
+    k_match<true, Q><<<grid, kMatchWarps * 32, smem>>>(plan, G, rows, t, nrows, cursor, out, limit, found, emb);
+  else
+    k_match<false, Q><<<grid, kMatchWarps * 32, smem>>>(plan, G, rows, t, nrows, cursor, out, limit, found, nullptr);
+  GPM_LAUNCH_CHECK();
+  return GPM_OK;
+}
+
+// Rows to aim for before the depth-first kernels start: about five per
+// resident warp (48 per SM).
+static int64_t row_target() { return (int64_t)num_sms() * 256; }
+
+// Breadth-first extension of a query's partial embeddings while they are
+// too few to fill the grid (small data graphs, rare labels, deep queries):
+// the rows of depth t (the (root, second vertex) pairs at t = 2) are extended
+// one position per step until there are at least `target` rows, t reaches
+// n - 1, or the next level would pass 2 GiB (or an eighth of the free
+// memory).  On return *rows, *nrows and *t describe the last level, held by
+// *store unless it is still the caller's; *nrows == 0: no embedding.
+static int extend_rows(const WidePlan &plan, const MatchGraph &G, DevBuf<int32_t> *store, const int32_t **rows,
+                       int64_t *nrows, int *t, int64_t target) {
+  if (*nrows == 0 || *nrows >= target || *t >= plan.n - 1) return GPM_OK;
+  size_t free_b = 0, total_b = 0;
+  GPM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const unsigned long long budget = std::min<unsigned long long>(2ull << 30, free_b / 8);
+  DevBuf<unsigned long long> cnt;
+  GPM_TRY(cnt.reserve(1));
+  const int blocks = num_sms() * 8;
+  while (*nrows > 0 && *nrows < target && *t < plan.n - 1) {
+    GPM_CUDA(cudaMemset(cnt.p, 0, 8));
+    k_extend_rows<<<blocks, 256>>>(plan, G, *rows, *nrows, *t, nullptr, 0, cnt.p);
+    GPM_LAUNCH_CHECK();
+    unsigned long long nn = 0;
+    GPM_CUDA(cudaMemcpy(&nn, cnt.p, 8, cudaMemcpyDeviceToHost));
+    if (nn * (unsigned long long)(*t + 1) * sizeof(int32_t) > budget) break;
+    DevBuf<int32_t> next;
+    if (nn) {
+      GPM_TRY(next.reserve((size_t)nn * (*t + 1)));
+      GPM_CUDA(cudaMemset(cnt.p, 0, 8));
+      k_extend_rows<<<blocks, 256>>>(plan, G, *rows, *nrows, *t, next.p, nn, cnt.p);
+      GPM_LAUNCH_CHECK();
+      GPM_CUDA(cudaDeviceSynchronize());  // the previous level is released below
+    }
+    *store = std::move(next);
+    *rows = store->p;
+    *nrows = (int64_t)nn;
+    ++*t;
+  }
+  return GPM_OK;
+}
 
 // The embeddings of q in g: counted (limit = ~0, emb = nullptr), counted up
 // to `limit`, or listed (emb: host array of limit * q->n ids).  *out = the
@@ -710,7 +888,7 @@ static int match_run(gpm_graph *g, const gpm_query *q, unsigned long long limit,
     GPM_CUDA(cudaMemcpy(hh.data(), h.p, sizeof(unsigned long long) * maxl, cudaMemcpyDeviceToHost));
     for (int i = 0; i < maxl; ++i) freq[i] = (int64_t)hh[i];
   }
-  QueryPlan plan;
+  WidePlan plan;
   GPM_TRY(plan_query(q, freq, &plan));
   DevBuf<unsigned long long> found;
   DevBuf<int32_t> demb;
@@ -758,25 +936,26 @@ static int match_run(gpm_graph *g, const gpm_query *q, unsigned long long limit,
     GPM_LAUNCH_CHECK();
     return finish(np);
   }
-  static PerDevice match_grid;
-  const int grid = match_grid.get([] {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match<false>, kMatchWarps * 32, 0);
-    return std::max(1, per_sm) * num_sms();
-  });
   const HubIndex hub{lc->hub_slot.p, lc->hub_bm.p, lc->hub_words};
+  const MatchGraph G{g->off.p, g->adj.p, lc->ladj.p, lc->loff.p, g->labels.p, lc->L, hub};
+  // the pairs are rows of two ids; too few of them are extended first
+  const int32_t *rows = reinterpret_cast<const int32_t *>(pairs.p);
+  int64_t nrows = (int64_t)np;
+  int t = 2;
+  DevBuf<int32_t> store;
+  GPM_TRY(extend_rows(plan, G, &store, &rows, &nrows, &t, row_target()));
+  if (nrows == 0) return finish(0);
   DevBuf<unsigned long long> cursor;
   GPM_TRY(cursor.reserve(1));
   GPM_CUDA(cudaMemset(cursor.p, 0, 8));
   GPM_CUDA(cudaMemset(d.p, 0, 8));
-  const MatchGraph G{g->off.p, g->adj.p, lc->ladj.p, lc->loff.p, g->labels.p, lc->L, hub};
-  if (track)
-    k_match<true><<<grid, kMatchWarps * 32>>>(plan, G, pairs.p, (int64_t)np, cursor.p, d.p, limit, found.p,
-                                              emb ? demb.p : nullptr);
-  else
-    k_match<false><<<grid, kMatchWarps * 32>>>(plan, G, pairs.p, (int64_t)np, cursor.p, d.p, limit, found.p,
-                                               nullptr);
-  GPM_LAUNCH_CHECK();
+  if (plan.n <= kNarrowQ) {
+    QueryPlan p16;
+    narrow_plan(plan, &p16);
+    GPM_TRY(launch_match(p16, G, rows, t, nrows, cursor.p, d.p, track, limit, found.p, emb ? demb.p : nullptr));
+  } else {
+    GPM_TRY(launch_match(plan, G, rows, t, nrows, cursor.p, d.p, track, limit, found.p, emb ? demb.p : nullptr));
+  }
   unsigned long long h = 0;
   GPM_CUDA(cudaMemcpy(&h, track ? found.p : d.p, 8, cudaMemcpyDeviceToHost));
   return finish(h);
@@ -817,14 +996,22 @@ int gpm_match_list(gpm_graph *g, const gpm_query *q, uint64_t limit, int32_t *em
 struct gpm_match_batch {
   gpm_graph *g = nullptr;
   int nq = 0, nm = 1;
-  std::vector<gpm::QueryPlan> plans;
+  int qcap = 16;  // plan width of the launch: 16, or 64 when a query has more than 16 vertices
+  std::vector<gpm::WidePlan> plans;
   std::vector<gpm::DevBuf<int2>> pairs;  // per query (empty for 1- and 2-vertex queries)
   std::vector<int64_t> npairs;
-  gpm::DevBuf<gpm::QueryPlan> dplans;
+  // per query: its task rows (the pairs, or their breadth-first extension
+  // held in ext), their count and depth
+  std::vector<gpm::DevBuf<int32_t>> ext;
+  std::vector<const int32_t *> rows;
+  std::vector<int64_t> nrows;
+  std::vector<int> depth;
+  gpm::DevBuf<int4> drows;               // nq x (rows pointer lo, hi, depth, -)
+  gpm::DevBuf<char> dplans;              // nq plans of width qcap
   gpm::DevBuf<int32_t> member;           // n (nm > 1 only)
   gpm::DevBuf<unsigned long long> base;  // counts of 1- and 2-vertex queries, nq * nm
   gpm::DevBuf<unsigned long long> out, cursor;
-  gpm::DevBuf<int4> tasks;
+  gpm::DevBuf<int4> tasks;               // (row index lo, hi, query, chunk or -1)
   int64_t ntasks = 0, span = 0;
   int grid = 0;  // persistent grid of k_match_batch
   cudaGraph_t graph = nullptr;
@@ -837,14 +1024,16 @@ struct gpm_match_batch {
 
 namespace gpm {
 
-__global__ void __launch_bounds__(kMatchWarps * 32)
-    k_match_batch(const QueryPlan *__restrict__ plans, MatchGraph G, const int4 *__restrict__ tasks, int64_t ntasks,
-                  int64_t span, const int32_t *__restrict__ member, int nm, unsigned long long *__restrict__ cursor,
-                  unsigned long long *__restrict__ out) {
-  __shared__ int32_t sbuf[kMatchWarps][kMaxQ][32];
-  __shared__ QueryPlan splan[kMatchWarps];
-  static_assert(sizeof(QueryPlan) % 4 == 0, "plan copied as words");
+template <int Q>
+__global__ void __launch_bounds__(kMatchWarps * 32, Q <= kNarrowQ ? GPM_MATCH_MIN_BLOCKS : 2)
+    k_match_batch(const QueryPlanT<Q> *__restrict__ plans, const int4 *__restrict__ qrows, MatchGraph G,
+                  const int4 *__restrict__ tasks, int64_t ntasks, int64_t span, const int32_t *__restrict__ member,
+                  int nm, unsigned long long *__restrict__ cursor, unsigned long long *__restrict__ out) {
+  __shared__ int32_t sbuf[kMatchWarps][Q <= kNarrowQ ? Q : 1][32];
+  __shared__ QueryPlanT<Q> splan[kMatchWarps];
+  static_assert(sizeof(QueryPlanT<Q>) % 4 == 0, "plan copied as words");
   const int w = threadIdx.x >> 5;
+  int32_t(*buf)[32] = warp_rows<Q>(sbuf[w]);
   const unsigned lane = lane_id();
   int cur = -1;
   while (true) {
@@ -857,40 +1046,46 @@ __global__ void __launch_bounds__(kMatchWarps * 32)
       __syncwarp();
       const int32_t *src = reinterpret_cast<const int32_t *>(plans + t.z);
       int32_t *dst = reinterpret_cast<int32_t *>(&splan[w]);
-      for (int i = lane; i < (int)(sizeof(QueryPlan) / 4); i += 32) dst[i] = src[i];
+      for (int i = lane; i < (int)(sizeof(QueryPlanT<Q>) / 4); i += 32) dst[i] = src[i];
       __syncwarp();
       cur = t.z;
     }
-    const unsigned long long c = match_task<false>(splan[w], G, t.x, t.y, t.w < 0 ? -1 : (int64_t)t.w * span, span,
-                                                   sbuf[w], ~0ull, nullptr, nullptr);
-    if (lane == 0 && c) atomicAdd(&out[(int64_t)t.z * nm + (member ? member[t.x] : 0)], c);
+    const int4 qr = qrows[t.z];
+    const int32_t *rows = reinterpret_cast<const int32_t *>(((unsigned long long)(unsigned)qr.y << 32) |
+                                                             (unsigned)qr.x);
+    const int32_t *row = rows + (((int64_t)t.y << 32) | (unsigned)t.x) * qr.z;
+    const unsigned long long c = match_task<false, Q>(splan[w], G, row, qr.z, t.w < 0 ? -1 : (int64_t)t.w * span,
+                                                      span, buf, ~0ull, nullptr, nullptr);
+    if (lane == 0 && c) atomicAdd(&out[(int64_t)t.z * nm + (member ? member[row[0]] : 0)], c);
   }
 }
 
-// Position 2's candidate count of each pair (the shortest label segment among
-// its mapped query-neighbours, as match_task opens it), as the task count of
-// the pair: ceil(len / span), at least 1.
-__global__ void k_pair_tasks(QueryPlan q, const int2 *__restrict__ pairs, int64_t np, const int64_t *__restrict__ off,
-                             const int32_t *__restrict__ loff, int L, int64_t span, int64_t *__restrict__ cnt) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t e[2] = {pairs[i].x, pairs[i].y};
-    const int lab = q.label[2];
-    int64_t best = -1;
-    const uint32_t nb = q.back_pos[2] | (1u << q.parent_pos[2]);
-    for (uint32_t bm = nb; bm; bm &= bm - 1) {
-      const int j = __ffs(bm) - 1;
-      int64_t s, en;
-      seg_range(off, loff, L, e[j], lab, &s, &en);
-      if (best < 0 || en - s < best) best = en - s;
-    }
+// Position t's candidate count of each row (the segment match_task opens:
+// the parent's label segment, or a shorter one of another mapped
+// query-neighbour when the lists are label-partitioned), as the task count of
+// the row: ceil(len / span), at least 1.
+__global__ void k_row_tasks(WidePlan q, const int32_t *__restrict__ rows, int64_t nrows, int t,
+                            const int64_t *__restrict__ off, const int32_t *__restrict__ loff, int L, int64_t span,
+                            int64_t *__restrict__ cnt) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t *row = rows + i * t;
+    const int lab = q.label[t];
+    int64_t s, e;
+    seg_range(off, loff, L, row[q.parent_pos[t]], lab, &s, &e);
+    int64_t best = e - s;
+    if (L > 0)
+      for (unsigned long long bm = q.back_pos[t]; bm; bm &= bm - 1) {
+        seg_range(off, loff, L, row[low_bit(bm)], lab, &s, &e);
+        best = min(best, e - s);
+      }
     cnt[i] = span > 0 ? max((int64_t)1, (best + span - 1) / span) : 1;
   }
 }
-__global__ void k_expand_tasks(const int2 *__restrict__ pairs, int64_t np, const int64_t *__restrict__ first,
-                               const int64_t *__restrict__ cnt, int query, int split, int4 *__restrict__ tasks) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x)
+__global__ void k_expand_tasks(int64_t nrows, const int64_t *__restrict__ first, const int64_t *__restrict__ cnt,
+                               int query, int split, int4 *__restrict__ tasks) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows; i += (int64_t)gridDim.x * blockDim.x)
     for (int64_t c = 0; c < cnt[i]; ++c)
-      tasks[first[i] + c] = make_int4(pairs[i].x, pairs[i].y, query, split ? (int)c : -1);
+      tasks[first[i] + c] = make_int4((int)(uint32_t)i, (int)(i >> 32), query, split ? (int)c : -1);
 }
 // per-member counts of a one-vertex query (vertices with its label) or of a
 // two-vertex query (its pairs, by the root's member)
@@ -931,15 +1126,16 @@ static int batch_tasks(gpm_match_batch *b, int64_t span) {
   std::vector<DevBuf<int64_t>> cnt(b->nq), first(b->nq);
   int64_t total = 0;
   const int blocks = num_sms() * 8;
+  // position t of a row is split into chunks only when the depth-first walk
+  // takes it (t <= n - 2; a row of depth n - 1 is closed at once)
+  auto splits = [&](int k) { return span > 0 && b->depth[k] <= b->plans[k].n - 2; };
   for (int k = 0; k < b->nq; ++k) {
-    const int64_t np = b->npairs[k];
+    const int64_t np = b->nrows[k];
     if (b->plans[k].n < 3 || np == 0) continue;
     GPM_TRY(cnt[k].reserve(np));
     GPM_TRY(first[k].reserve(np + 1));
-    if (b->plans[k].n >= 4)
-      k_pair_tasks<<<blocks, 256>>>(b->plans[k], b->pairs[k].p, np, g->off.p, lc->loff.p, lc->L, span, cnt[k].p);
-    else
-      k_pair_tasks<<<blocks, 256>>>(b->plans[k], b->pairs[k].p, np, g->off.p, lc->loff.p, lc->L, 0, cnt[k].p);
+    k_row_tasks<<<blocks, 256>>>(b->plans[k], b->rows[k], np, b->depth[k], g->off.p, lc->loff.p, lc->L,
+                                 splits(k) ? span : 0, cnt[k].p);
     GPM_LAUNCH_CHECK();
     size_t tmp = 0;
     cub::DeviceScan::InclusiveSum(nullptr, tmp, cnt[k].p, first[k].p + 1, (int)np);
@@ -957,8 +1153,7 @@ static int batch_tasks(gpm_match_batch *b, int64_t span) {
   for (int k = 0; k < b->nq; ++k) {
     if (!cnt_total[k]) continue;
     // each query's tasks at its own offset: shift the scan by `at`
-    k_expand_tasks<<<blocks, 256>>>(b->pairs[k].p, b->npairs[k], first[k].p, cnt[k].p, k,
-                                    b->plans[k].n >= 4 && span > 0, b->tasks.p + at);
+    k_expand_tasks<<<blocks, 256>>>(b->nrows[k], first[k].p, cnt[k].p, k, splits(k), b->tasks.p + at);
     GPM_LAUNCH_CHECK();
     at += cnt_total[k];
   }
@@ -969,11 +1164,14 @@ static int batch_tasks(gpm_match_batch *b, int64_t span) {
   return GPM_OK;
 }
 
+template <int Q>
 static int batch_grid() {
   static PerDevice grid;
   return grid.get([] {
+    constexpr int smem = match_dyn_smem<Q>();
+    if (smem > 0) cudaFuncSetAttribute(k_match_batch<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_batch, kMatchWarps * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_batch<Q>, kMatchWarps * 32, smem);
     return std::max(1, per_sm) * num_sms();
   });
 }
@@ -987,9 +1185,15 @@ static int batch_launch(gpm_match_batch *b, cudaStream_t st) {
   if (b->ntasks == 0) return GPM_OK;
   const MatchGraph G{g->off.p, g->adj.p, lc->ladj.p, lc->loff.p, g->labels.p, lc->L,
                      HubIndex{lc->hub_slot.p, lc->hub_bm.p, lc->hub_words}};
-  k_match_batch<<<b->grid, kMatchWarps * 32, 0, st>>>(b->dplans.p, G, b->tasks.p, b->ntasks, b->span,
-                                                                 b->nm > 1 ? b->member.p : nullptr, b->nm, b->cursor.p,
-                                                                 b->out.p);
+  const int32_t *member = b->nm > 1 ? b->member.p : nullptr;
+  if (b->qcap <= kNarrowQ)
+    k_match_batch<kNarrowQ><<<b->grid, kMatchWarps * 32, 0, st>>>(
+        reinterpret_cast<const QueryPlan *>(b->dplans.p), b->drows.p, G, b->tasks.p, b->ntasks, b->span, member,
+        b->nm, b->cursor.p, b->out.p);
+  else
+    k_match_batch<kMaxQ><<<b->grid, kMatchWarps * 32, match_dyn_smem<kMaxQ>(), st>>>(
+        reinterpret_cast<const WidePlan *>(b->dplans.p), b->drows.p, G, b->tasks.p, b->ntasks, b->span, member,
+        b->nm, b->cursor.p, b->out.p);
   GPM_LAUNCH_CHECK();
   return GPM_OK;
 }
@@ -1053,19 +1257,28 @@ int gpm_match_batch_create(gpm_graph *g, int nq, const gpm_query *const *queries
   if ((s = ensure_label_csr(g))) return bail(s);
   LabelCsr *lc = g->lcsr;
   const size_t cells = (size_t)nq * b->nm;
+  for (int k = 0; k < nq; ++k)
+    if (queries[k]->n > kNarrowQ) b->qcap = kMaxQ;
+  const size_t plan_bytes = b->qcap <= kNarrowQ ? sizeof(QueryPlan) : sizeof(WidePlan);
   if ((s = b->base.reserve(cells)) || (s = b->out.reserve(cells)) || (s = b->cursor.reserve(1)) ||
-      (s = b->dplans.reserve(nq)))
+      (s = b->dplans.reserve(plan_bytes * nq)))
     return bail(s);
   GPM_CUDA(cudaMemset(b->base.p, 0, sizeof(unsigned long long) * cells));
   b->plans.resize(nq);
   b->pairs.resize(nq);
   b->npairs.assign(nq, 0);
+  b->ext.resize(nq);
+  b->rows.assign(nq, nullptr);
+  b->nrows.assign(nq, 0);
+  b->depth.assign(nq, 2);
+  const MatchGraph G{g->off.p, g->adj.p, lc->ladj.p, lc->loff.p, g->labels.p, lc->L,
+                     HubIndex{lc->hub_slot.p, lc->hub_bm.p, lc->hub_words}};
   DevBuf<unsigned long long> np;
   if ((s = np.reserve(1))) return bail(s);
   const int blocks = (int)std::min<int64_t>((g->n * 32 + 255) / 256, (int64_t)num_sms() * 16);
   const int sblocks = (int)std::min<int64_t>((g->n + 255) / 256 + 1, (int64_t)num_sms() * 8);
   for (int k = 0; k < nq; ++k) {
-    QueryPlan &p = b->plans[k];
+    WidePlan &p = b->plans[k];
     if ((s = plan_query(queries[k], freq, &p))) return bail(s);
     if (p.n == 1) {
       if (g->n) k_small_counts<<<sblocks, 256>>>(g->n, g->labels.p, p.label[0], nullptr, 0,
@@ -1082,12 +1295,34 @@ int gpm_match_batch_create(gpm_graph *g, int nq, const gpm_query *const *queries
     GPM_CUDA(cudaMemset(np.p, 0, 8));
     k_match_pairs<<<blocks, 256>>>(p, g->n, g->off.p, lc->ladj.p, lc->loff.p, lc->L, g->labels.p, 0, b->pairs[k].p,
                                    np.p);
-    if (p.n == 2)
+    if (p.n == 2) {
       k_small_counts<<<sblocks, 256>>>(0, nullptr, 0, b->pairs[k].p, (int64_t)h, b->nm > 1 ? b->member.p : nullptr,
                                        b->base.p + (size_t)k * b->nm);
+      continue;
+    }
+    // the pairs are rows of two ids; too few of them are extended first
+    b->rows[k] = reinterpret_cast<const int32_t *>(b->pairs[k].p);
+    b->nrows[k] = (int64_t)h;
+    if ((s = extend_rows(p, G, &b->ext[k], &b->rows[k], &b->nrows[k], &b->depth[k], row_target()))) return bail(s);
   }
-  GPM_CUDA(cudaMemcpy(b->dplans.p, b->plans.data(), sizeof(QueryPlan) * nq, cudaMemcpyHostToDevice));
-  b->grid = batch_grid();
+  {
+    std::vector<int4> qr(nq);
+    for (int k = 0; k < nq; ++k) {
+      const unsigned long long a = (unsigned long long)(uintptr_t)b->rows[k];
+      qr[k] = make_int4((int)(uint32_t)a, (int)(uint32_t)(a >> 32), b->depth[k], 0);
+    }
+    if ((s = b->drows.reserve(nq))) return bail(s);
+    GPM_CUDA(cudaMemcpy(b->drows.p, qr.data(), sizeof(int4) * nq, cudaMemcpyHostToDevice));
+  }
+  if (b->qcap <= kNarrowQ) {
+    std::vector<QueryPlan> narrow(nq);
+    for (int k = 0; k < nq; ++k) narrow_plan(b->plans[k], &narrow[k]);
+    GPM_CUDA(cudaMemcpy(b->dplans.p, narrow.data(), plan_bytes * nq, cudaMemcpyHostToDevice));
+    b->grid = batch_grid<kNarrowQ>();
+  } else {
+    GPM_CUDA(cudaMemcpy(b->dplans.p, b->plans.data(), plan_bytes * nq, cudaMemcpyHostToDevice));
+    b->grid = batch_grid<kMaxQ>();
+  }
   if ((s = batch_tasks(b, 0))) return bail(s);
   *out = b;
   return GPM_OK;

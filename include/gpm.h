@@ -321,7 +321,9 @@ int gpm_batch_motif_async(gpm_batch *b, int use_graph, void *stream, uint64_t *d
 int gpm_batch_destroy(gpm_batch *b);
 
 /* ---- labelled subgraph matching (sub_ceci semantics) ----------------------- */
-/* Query graph: n vertices (n <= 16), m undirected edges listed once, labels. */
+/* Query graph: n vertices (1 <= n <= 64, sub_ceci's MAX_QUERY_VERTEX in
+ * sub_ceci/configuration/config.h:12), m undirected edges listed once,
+ * labels.  n > 64 fails with GPM_EUNSUPPORTED. */
 int gpm_query_create(int64_t n, int64_t m, const int32_t *src, const int32_t *dst,
                      const int32_t *labels, gpm_query **out);
 int gpm_query_destroy(gpm_query *q);
@@ -348,13 +350,14 @@ typedef struct gpm_match_batch gpm_match_batch;
  * persistent launch (sub_ceci semantics, as gpm_match).  member (host, n ids
  * in [0, nmembers), may be NULL) names each vertex's member when the data
  * graph is a disjoint union of many graphs: each embedding is counted for its
- * root's member.  The plan (each query's (root, second vertex) tasks) is
- * built here; `data` must outlive the batch. */
+ * root's member.  The plan (each query's (root, second vertex) tasks,
+ * extended breadth first to longer partial embeddings where they are too few
+ * to fill the GPU) is built here; `data` must outlive the batch. */
 int gpm_match_batch_create(gpm_graph *data, int nq, const gpm_query *const *queries, const int32_t *member,
                            int nmembers, gpm_match_batch **out);
 /* Chooses how finely tasks of queries with 4 or more vertices are split (the
- * span of position-2 candidates per task; 0 = unsplit) by timing candidates;
- * *span (may be NULL) receives it. */
+ * span of candidates of a task's first unmapped position per task; 0 =
+ * unsplit) by timing candidates; *span (may be NULL) receives it. */
 int gpm_match_batch_autotune(gpm_match_batch *b, int64_t *span);
 /* Counts: out[q * nmembers + m] (host, nq * nmembers uint64, nmembers = 1
  * without member ids).  use_graph != 0 captures the launch into a CUDA graph

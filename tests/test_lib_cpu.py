@@ -104,6 +104,17 @@ def test_device_calls_fail_cleanly_without_gpu():
     assert e.value.status == 7
 
 
+def test_query_size_limit():
+    """Query graphs of up to 64 vertices are accepted (sub_ceci's
+    MAX_QUERY_VERTEX, sub_ceci/configuration/config.h:12); 65 is refused."""
+    path = np.arange(63, dtype=np.int32)
+    q = gpm.Query(64, path, path + 1, np.zeros(64, np.int32))
+    q.close()
+    with pytest.raises(gpm.GpmError) as e:
+        gpm.Query(65, path, path + 1, np.zeros(65, np.int32))
+    assert "64" in str(e.value)
+
+
 def test_oracle_generators_match_the_engine():
     # bench.py's reference arm and the fixture scripts build their graphs with
     # the oracle's restated generators so that they never load the engine;

@@ -75,7 +75,7 @@ def test_single_vertex_and_errors():
     g = gpm.Graph.from_edges(4, [0, 1], [1, 2], labels=[1, 1, 2, 1])
     assert g.match(gpm.Query(1, [], [], [1])) == 3
     with pytest.raises(gpm.GpmError):
-        gpm.Query(17, [0], [1], np.zeros(17))
+        gpm.Query(65, [0], [1], np.zeros(65))
     g2 = gpm.Graph.from_edges(4, [0, 1], [1, 2])
     with pytest.raises(gpm.GpmError):
         g2.match(gpm.Query(2, [0], [1], [0, 0]))

@@ -64,6 +64,26 @@ def test_reference_subceci_on_random_graphs():
         assert orc.match(off, idx, lab, qo, qi, ql) == int(row[-1]), (gi, si)
 
 
+def test_reference_subceci_wide_queries():
+    """Query graphs of 16..64 vertices: the oracle equals the counts the
+    reference's own sub_ceci printed (ceci_wide.npz)."""
+    z = np.load(os.path.join(GOLD, "ceci_wide.npz"))
+    gs = np.concatenate([[0], np.cumsum(z["ge_len"])])
+    ls = np.concatenate([[0], np.cumsum(z["gn"])])
+    qs = np.concatenate([[0], np.cumsum(z["q_e_len"])])
+    qls = np.concatenate([[0], np.cumsum(z["q_n"])])
+    assert len(z["q_n"]) >= 60 and int(z["q_n"].max()) == 64
+    for i in range(len(z["q_n"])):
+        gi = int(z["q_graph"][i])
+        e = z["ge"][gs[gi]: gs[gi + 1]]
+        off, idx = orc.build_csr(int(z["gn"][gi]), e[:, 0], e[:, 1])
+        k = int(z["q_n"][i])
+        qe = z["q_e"][qs[i]: qs[i + 1]]
+        qo, qi = orc.build_csr(k, qe[:, 0], qe[:, 1])
+        got = orc.match(off, idx, z["gl"][ls[gi]: ls[gi + 1]], qo, qi, z["q_lab"][qls[i]: qls[i + 1]])
+        assert got == int(z["expected"][i]), i
+
+
 def test_sample_dataset_counts():
     z = np.load(os.path.join(GOLD, "ref_small.npz"))
     off, idx = orc.build_csr(5, z["sample_e"][:, 0], z["sample_e"][:, 1])
