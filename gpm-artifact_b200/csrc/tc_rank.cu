@@ -53,19 +53,24 @@ static int grid_for(int64_t work, int block = 256) {
 }
 
 // ------------------------------------------------------------ membership
-// Every key handed to a table lies in [min N(owner), max N(owner)]: the plan
-// clipped the partner segments to that range, so the maps need no range
-// check.
+// Keys handed to a table come from aligned 16-byte rows of the padded lists
+// (radj4): the clipped segment's own keys lie in [min N(owner), max
+// N(owner)], and the other keys of its first and last rows lie below that
+// range (earlier keys of the sorted partner list) or above it (later keys,
+// the INT32_MAX padding).  The byte map and bitmap clamp the key's offset to
+// the span, where a guard entry is zero; the hash table finds no such key.
 struct ByteTable {
-  const uint8_t *bm;
+  const uint8_t *bm;  // span + 1 bytes, bm[span] = 0
   int32_t base;
-  __device__ __forceinline__ unsigned hit(int32_t w) const { return bm[w - base]; }
+  uint32_t span;
+  __device__ __forceinline__ unsigned hit(int32_t w) const { return bm[min((uint32_t)(w - base), span)]; }
 };
 struct BitTable {
-  const uint32_t *bm;
+  const uint32_t *bm;  // span + 1 bits, bit span = 0
   int32_t base;
+  uint32_t span;
   __device__ __forceinline__ unsigned hit(int32_t w) const {
-    uint32_t o = (uint32_t)(w - base);
+    const uint32_t o = min((uint32_t)(w - base), span);
     return (bm[o >> 5] >> (o & 31)) & 1u;
   }
 };
@@ -84,35 +89,45 @@ struct HashTable {
   }
 };
 
-// Segments of one owner: the long ones [l0, l1): each half-warp streams one,
-// 16 keys per step (each step one coalesced 64-byte row), so the
-// per-segment work of a warp is shared by two segments; the short ones
-// [s0, s1): 8-lane groups, four segments per warp.  `wid`/`nw` spread segments
-// over the warps of the executing group (1 warp for warp tasks, the CTA's
-// warps for CTA tasks).  R-MAT 22: half-warps 7.0 ms against 7.6 ms for
-// whole-warp streaming of the same segments.
+#ifndef GPM_RANK_UNROLL
+#define GPM_RANK_UNROLL 1
+#endif
+constexpr int kRankUnroll = GPM_RANK_UNROLL;  // 16-byte rows in flight per lane
 template <class T>
-__device__ __forceinline__ unsigned long long scan_segments(const int32_t *__restrict__ radj,
+__device__ __forceinline__ unsigned hit4(const T &t, int4 v) {
+  return t.hit(v.x) + t.hit(v.y) + t.hit(v.z) + t.hit(v.w);
+}
+
+// Segments of one owner, read as aligned 16-byte rows of radj4 (four keys
+// per lane and load; the rows' keys outside the segment miss, see above):
+// the long ones [l0, l1): each half-warp streams one, 64 keys per step (one
+// 256-byte row), so the per-segment work of a warp is shared by two
+// segments; the short ones [s0, s1): 8-lane groups, four segments per warp.
+// `wid`/`nw` spread segments over the warps of the executing group (1 warp
+// for warp tasks, the CTA's warps for CTA tasks).
+template <class T>
+__device__ __forceinline__ unsigned long long scan_segments(const int32_t *__restrict__ radj4,
                                                             const longlong2 *__restrict__ pseg, int64_t l0,
                                                             int64_t l1, int64_t s0, int64_t s1, const T &t,
                                                             int wid, int nw, unsigned lane) {
+  const int4 *__restrict__ rows = reinterpret_cast<const int4 *>(radj4);
   unsigned long long c = 0;
   int64_t j;
   const unsigned half = lane >> 4, hl = lane & 15;
   for (j = l0 + wid * 2 + half; j < l1; j += nw * 2) {
     const longlong2 sg = pseg[j];
-    const int32_t *__restrict__ q = radj + sg.x;
-    const int len = (int)(sg.y - sg.x);
+    const int4 *__restrict__ q = rows + (sg.x >> 2);
+    const int nr = (int)(((sg.y + 3) >> 2) - (sg.x >> 2));
     unsigned cs = 0;
-#pragma unroll 4
-    for (int i = (int)hl; i < len; i += 16) cs += t.hit(__ldg(q + i));
+#pragma unroll kRankUnroll
+    for (int i = (int)hl; i < nr; i += 16) cs += hit4(t, __ldg(q + i));
     c += cs;
   }
   const unsigned grp = lane >> 3, gl = lane & 7;
   for (j = s0 + wid * 4 + grp; j < s1; j += nw * 4) {
     const longlong2 sg = pseg[j];
     unsigned cs = 0;
-    for (int64_t k = sg.x + gl; k < sg.y; k += 8) cs += t.hit(__ldg(radj + k));
+    for (int64_t k = (sg.x >> 2) + gl; k < (sg.y + 3) >> 2; k += 8) cs += hit4(t, __ldg(rows + k));
     c += cs;
   }
   return c;
@@ -138,6 +153,7 @@ __device__ __forceinline__ void group_sync() {
 template <bool CTA, bool REC>
 __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_t *__restrict__ roff,
                                                          const int32_t *__restrict__ radj,
+                                                         const int32_t *__restrict__ radj4,
                                                          const int64_t *__restrict__ poff,
                                                          const longlong2 *__restrict__ pseg,
                                                          const int32_t *__restrict__ plong,
@@ -153,16 +169,17 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
   const int32_t kmin = radj[s0], kmax = radj[s0 + d - 1];
   const int64_t span = (int64_t)kmax - kmin + 1;
   unsigned long long c = 0;
-  if (span <= (int64_t)nwords * 4) {
-    const int nclear = (int)((span + 3) >> 2);
+  // byte map / bitmap: span + 1 entries, the last the zero guard
+  if (span < (int64_t)nwords * 4) {
+    const int nclear = (int)((span + 4) >> 2);
     for (int i = tid; i < nclear; i += nthr) words[i] = 0u;
     group_sync<CTA>();
     uint8_t *bytes = reinterpret_cast<uint8_t *>(words);
     for (int i = tid; i < d; i += nthr) bytes[radj[s0 + i] - kmin] = 1;
     group_sync<CTA>();
-    c = scan_segments(radj, pseg, l0, l1, h0, h1, ByteTable{bytes, kmin}, wid, nw, lane);
-  } else if (span <= (int64_t)nwords * 32) {
-    const int nclear = (int)((span + 31) >> 5);
+    c = scan_segments(radj4, pseg, l0, l1, h0, h1, ByteTable{bytes, kmin, (uint32_t)span}, wid, nw, lane);
+  } else if (span < (int64_t)nwords * 32) {
+    const int nclear = (int)((span + 32) >> 5);
     for (int i = tid; i < nclear; i += nthr) words[i] = 0u;
     group_sync<CTA>();
     for (int i = tid; i < d; i += nthr) {
@@ -170,7 +187,7 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
       atomicOr(&words[o >> 5], 1u << (o & 31));
     }
     group_sync<CTA>();
-    c = scan_segments(radj, pseg, l0, l1, h0, h1, BitTable{words, kmin}, wid, nw, lane);
+    c = scan_segments(radj4, pseg, l0, l1, h0, h1, BitTable{words, kmin, (uint32_t)span}, wid, nw, lane);
   } else {
     int32_t *tab = reinterpret_cast<int32_t *>(words);
     const int logcap = 31 - __clz(nwords);
@@ -187,7 +204,7 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
         while (atomicCAS(&tab[h], -1, key) != -1) h = (h + 1) & mask;
       }
       group_sync<CTA>();
-      c += scan_segments(radj, pseg, l0, l1, h0, h1, HashTable{tab, logcap}, wid, nw, lane);
+      c += scan_segments(radj4, pseg, l0, l1, h0, h1, HashTable{tab, logcap}, wid, nw, lane);
     }
   }
   if (REC && lane == 0) atomicAdd(rec, (unsigned long long)(clock64() - t0));
@@ -207,7 +224,8 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
 template <bool REC>
 __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     k_tc_rank_t(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
+                const int32_t *__restrict__ radj4, const int64_t *__restrict__ poff,
+                const longlong2 *__restrict__ pseg,
                 const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
                 const int32_t *__restrict__ cta_tasks, int n_cta,
                 const int32_t *__restrict__ warp_tasks, int n_warp, int *__restrict__ counters,
@@ -222,7 +240,8 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     __syncthreads();
     if (t >= n_cta) break;
     const int32_t x = cta_tasks[t];
-    c += owner_task<true, REC>(x, roff, radj, poff, pseg, plong, pshort, rsm, kCtaWords, REC ? rec + x : nullptr);
+    c += owner_task<true, REC>(x, roff, radj, radj4, poff, pseg, plong, pshort, rsm, kCtaWords,
+                               REC ? rec + x : nullptr);
   }
   const int wid = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31;
@@ -233,7 +252,8 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= n_warp) break;
     const int32_t x = warp_tasks[t];
-    c += owner_task<false, REC>(x, roff, radj, poff, pseg, plong, pshort, region, kWarpWords, REC ? rec + x : nullptr);
+    c += owner_task<false, REC>(x, roff, radj, radj4, poff, pseg, plong, pshort, region, kWarpWords,
+                                REC ? rec + x : nullptr);
   }
   c = warp_sum(c);
   if (lane == 0 && c) atomicAdd(out, c);
@@ -400,13 +420,15 @@ __device__ __forceinline__ int64_t upper_bound_key(const int32_t *__restrict__ a
 // closes no triangle through the edge).  It goes into the owner's room
 // [poff[x], poff[x+1]) -- one slot per incident edge, so it always fits --
 // long segments from the front (cursor plong[x]), short ones from the back
-// (cursor pshort[x]).  upward: every list holds only ids above its vertex,
+// (cursor pshort[x]), as ranges of radj4.  With radj4 non-null the pass also
+// copies each list u into it (with its INT32_MAX padding).  upward: every list holds only ids above its vertex,
 // so when u owns the edge, min N(u) <= v < every id of N(v) and the lower
 // search is skipped.  The lanes of a warp that share an (owner, class) take
 // their slots with one atomic (hub owners get most of theirs from their own
 // list, i.e. from one warp).
 __global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                                int upward, int long_min, const uint8_t *__restrict__ cfg,
+                                const int64_t *__restrict__ roff4, int32_t *__restrict__ radj4, int upward,
+                                int long_min, const uint8_t *__restrict__ cfg,
                                 const int64_t *__restrict__ poff, int32_t *__restrict__ plong,
                                 int32_t *__restrict__ pshort, longlong2 *__restrict__ pseg,
                                 unsigned long long *__restrict__ work) {
@@ -414,6 +436,14 @@ __global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, con
   int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = warp; u < n; u += nw) {
     int64_t s = roff[u], e = roff[u + 1], du = e - s;
+    if (radj4) {  // u's list into radj4 with its padding, one 16-byte row per lane
+      int4 *row = reinterpret_cast<int4 *>(radj4 + roff4[u]);
+      for (int64_t r = lane_id(); 4 * r < du; r += 32) {
+        const int64_t b = s + 4 * r;
+        row[r] = make_int4(radj[b], b + 1 < e ? radj[b + 1] : INT32_MAX, b + 2 < e ? radj[b + 2] : INT32_MAX,
+                           b + 3 < e ? radj[b + 3] : INT32_MAX);
+      }
+    }
     for (int64_t k = s + lane_id(); k < e; k += 32) {
       int32_t v = radj[k];
       int64_t vs = roff[v], ve = roff[v + 1], dv = ve - vs;
@@ -435,12 +465,21 @@ __global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, con
       if (grp.thread_rank() == 0) base = atomicAdd(lng ? &plong[owner] : &pshort[owner], (int)grp.size());
       const int64_t slot = grp.shfl(base, 0) + (int64_t)grp.thread_rank();
       const int64_t pos = lng ? poff[owner] + slot : poff[owner + 1] - 1 - slot;
-      pseg[pos] = make_longlong2(lo, lo + len);
+      const int32_t partner = own_u ? v : (int32_t)u;
+      const int64_t lo4 = lo - roff[partner] + roff4[partner];  // the same keys in radj4
+      pseg[pos] = make_longlong2(lo4, lo4 + len);
       const unsigned long long w = cg::reduce(grp, (unsigned long long)len + 1ull, cg::plus<unsigned long long>());
       if (grp.thread_rank() == 0) atomicAdd(&work[owner], w);
     }
   }
 }
+// roff4: list lengths rounded up to a multiple of four, for the scan that
+// places every list of radj4 at a multiple of four keys
+__global__ void k_padded_len(int64_t n, const int64_t *__restrict__ roff, int64_t *__restrict__ len4) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    len4[v] = (roff[v + 1] - roff[v] + 3) & ~(int64_t)3;
+}
+
 // tasks: owners with partners; key = ~work so an ascending sort puts heavy first
 __global__ void k_rank_tasks(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ plong,
                              const int32_t *__restrict__ pshort,
@@ -841,8 +880,29 @@ int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st) {
   return GPM_OK;
 }
 
+// roff4 of the rank graph and room for radj4 (kept with it); *fill: radj4
+// is still empty and the next placement pass writes it.  radj4 takes at
+// most nnz + 3n keys, so no count is read back.
+static int ensure_padded_lists(gpm_graph *g, cudaStream_t st, bool *fill) {
+  RankGraph *r = g->rg;
+  *fill = false;
+  if (r->padded) return GPM_OK;
+  const int64_t n = g->n;
+  DevBuf<int64_t> len4;
+  GPM_TRY(len4.reserve(std::max<int64_t>(n, 1)));
+  GPM_TRY(r->roff4.reserve(n + 1));
+  GPM_TRY(r->radj4.reserve(r->radj.n + 3 * (size_t)n + 4));  // radj.n: the rank graph's stored keys
+  k_padded_len<<<grid_for(n), 256, 0, st>>>(n, r->roff.p, len4.p);
+  GPM_LAUNCH_CHECK();
+  GPM_TRY(scan_i64(n, len4.p, r->roff4.p, st));
+  *fill = true;
+  return GPM_OK;
+}
+
 int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, cudaStream_t st, RankPlan **out) {
   GPM_TRY(ensure_rank_graph(g, st));
+  bool fill = false;
+  GPM_TRY(ensure_padded_lists(g, st, &fill));
   const int64_t n = g->n;
   RankPlan *p = new RankPlan();
   p->cta_min = cta_min;
@@ -865,8 +925,11 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
   cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(p->pshort.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
-  k_partner_place<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, g->rg->upward, long_min, cfg, p->poff.p,
-                                                     p->plong.p, p->pshort.p, p->pseg.p, work.p);
+  k_partner_place<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, g->rg->roff4.p, fill ? g->rg->radj4.p : nullptr,
+                                                     g->rg->upward, long_min, cfg, p->poff.p, p->plong.p, p->pshort.p,
+                                                     p->pseg.p, work.p);
+  GPM_LAUNCH_CHECK();
+  if (fill) g->rg->padded = 1;
   // 3. task queues, heaviest first
   DevBuf<unsigned long long> ckey, wkey;
   DevBuf<int32_t> cval, wval;
@@ -908,11 +971,13 @@ int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long l
   if (g->nnz == 0) return GPM_OK;
   GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 4 * sizeof(int), st));
   if (rec)
-    k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p,
+    k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, g->rg->radj4.p,
+                                                           p->poff.p, p->pseg.p,
                                                            p->plong.p, p->pshort.p, p->cta_tasks.p, p->n_cta, p->warp_tasks.p,
                                                            p->n_warp, p->counters.p, d_out, rec);
   else
-    k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p, p->plong.p,
+    k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, g->rg->radj4.p, p->poff.p,
+                                                   p->pseg.p, p->plong.p,
                                                    p->pshort.p,
                                                    p->cta_tasks.p, p->n_cta, p->warp_tasks.p, p->n_warp,
                                                    p->counters.p, d_out, nullptr);

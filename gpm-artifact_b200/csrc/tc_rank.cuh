@@ -21,10 +21,11 @@ constexpr int kRankCtaWords = GPM_RANK_CTA_WORDS;
 #endif
 constexpr int kRankCtaMin = GPM_RANK_CTA_MIN;
 // fixed schedule: partner segments of at least this many keys are streamed
-// by a half-warp, shorter ones by 8-lane groups (R-MAT 20: 1.35 ms at 64,
-// 1.38 ms at 32)
+// by a half-warp, shorter ones by 8-lane groups (16-byte rows, R-MAT 22:
+// 6.63 ms at 32, 6.66 at 24 and 128, 6.70 at 48, 6.72 at 64; every segment
+// to 8-lane groups 7.17 ms)
 #ifndef GPM_RANK_LONG_MIN
-#define GPM_RANK_LONG_MIN 64
+#define GPM_RANK_LONG_MIN 32
 #endif
 constexpr int kRankLongMin = GPM_RANK_LONG_MIN;
 
@@ -41,6 +42,15 @@ struct RankGraph {
   DevBuf<int64_t> rinc;
   int64_t nin = 0;
   int upward = 0;
+  // The lists again, each padded with INT32_MAX to a multiple of four keys
+  // and starting at a multiple of four (roff4), for the count kernel's
+  // 16-byte loads: an aligned 16-byte row of a clipped partner segment then
+  // stays inside its list, and the keys it holds outside the segment lie
+  // below the owner's smallest key or above its largest (built with the
+  // first triangle plan)
+  DevBuf<int64_t> roff4;
+  DevBuf<int32_t> radj4;
+  int padded = 0;  // radj4 written
 };
 
 // Per-graph schedule of GPM_TC_BITMAP (device arrays):
@@ -48,9 +58,9 @@ struct RankGraph {
 //               poff[x+1]) (poff = rinc, one slot per incident edge); its
 //               plong[x] long segments fill the room from the front, its
 //               pshort[x] short ones from the back.  A segment is the
-//               [start, end) range of radj holding the part of one partner's
-//               list inside [min N(x), max N(x)] (no key outside that range
-//               can be in N(x)); empty ranges are left out
+//               [start, end) range of radj4 holding the part of one
+//               partner's list inside [min N(x), max N(x)] (no key outside
+//               that range can be in N(x)); empty ranges are left out
 //   cta_tasks / warp_tasks  owners by size class, heaviest first
 struct RankPlan {
   int cta_min = 0, long_min = 0;
