@@ -89,6 +89,9 @@ struct HashTable {
   }
 };
 
+#ifndef GPM_RANK_SHORT_LANES
+#define GPM_RANK_SHORT_LANES 4  // lanes per short segment (2, 4, 8 or 16)
+#endif
 #ifndef GPM_RANK_UNROLL
 #define GPM_RANK_UNROLL 1
 #endif
@@ -102,7 +105,8 @@ __device__ __forceinline__ unsigned hit4(const T &t, int4 v) {
 // per lane and load; the rows' keys outside the segment miss, see above):
 // the long ones [l0, l1): each half-warp streams one, 64 keys per step (one
 // 256-byte row), so the per-segment work of a warp is shared by two
-// segments; the short ones [s0, s1): 8-lane groups, four segments per warp.
+// segments; the short ones [s0, s1): groups of GPM_RANK_SHORT_LANES lanes,
+// eight segments per warp at 4 lanes.
 // `wid`/`nw` spread segments over the warps of the executing group (1 warp
 // for warp tasks, the CTA's warps for CTA tasks).
 template <class T>
@@ -123,11 +127,12 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
     for (int i = (int)hl; i < nr; i += 16) cs += hit4(t, __ldg(q + i));
     c += cs;
   }
-  const unsigned grp = lane >> 3, gl = lane & 7;
-  for (j = s0 + wid * 4 + grp; j < s1; j += nw * 4) {
+  constexpr int S = GPM_RANK_SHORT_LANES, G = 32 / S;
+  const unsigned grp = lane / S, gl = lane % S;
+  for (j = s0 + wid * G + grp; j < s1; j += nw * G) {
     const longlong2 sg = pseg[j];
     unsigned cs = 0;
-    for (int64_t k = (sg.x >> 2) + gl; k < (sg.y + 3) >> 2; k += 8) cs += hit4(t, __ldg(rows + k));
+    for (int64_t k = (sg.x >> 2) + gl; k < (sg.y + 3) >> 2; k += S) cs += hit4(t, __ldg(rows + k));
     c += cs;
   }
   return c;

@@ -21,11 +21,12 @@ constexpr int kRankCtaWords = GPM_RANK_CTA_WORDS;
 #endif
 constexpr int kRankCtaMin = GPM_RANK_CTA_MIN;
 // fixed schedule: partner segments of at least this many keys are streamed
-// by a half-warp, shorter ones by 8-lane groups (16-byte rows, R-MAT 22:
-// 6.63 ms at 32, 6.66 at 24 and 128, 6.70 at 48, 6.72 at 64; every segment
-// to 8-lane groups 7.17 ms)
+// by a half-warp, shorter ones by 4-lane groups (16-byte rows, R-MAT 22:
+// 6.47-6.49 ms at 16, 6.53 at 8, 6.51-6.57 at 24; with 8-lane groups 6.63 ms
+// at 32, 6.66 at 24 and 128, 6.72 at 64; 2-lane groups 6.52 ms at 8 or 16;
+// every segment to 8-lane groups 7.17 ms)
 #ifndef GPM_RANK_LONG_MIN
-#define GPM_RANK_LONG_MIN 32
+#define GPM_RANK_LONG_MIN 16
 #endif
 constexpr int kRankLongMin = GPM_RANK_LONG_MIN;
 
