@@ -348,9 +348,10 @@ def tc_line(args, rank, world, dist, local):
     wedge, pair = g.work()
     bytes_graded = 4 * (n + 1) + 4 * m_und + 4 * wedge
     # bytes this kernel requests: the clipped segments (4 B a key, a 16-byte
-    # descriptor each), every owner list once, 36 B of offsets and counts per owner
-    nseg, seg_keys, owner_keys, ntasks = g.plan_stats()
-    bytes_req = 4 * seg_keys + 16 * nseg + 4 * owner_keys + 36 * ntasks
+    # descriptor each), the core-row words of the dense segments (4 B each),
+    # every owner list once, 36 B of offsets and counts per owner
+    nseg, seg_keys, owner_keys, ntasks, dense_segs, dense_words = g.plan_stats()
+    bytes_req = 4 * seg_keys + 4 * dense_words + 16 * nseg + 4 * owner_keys + 36 * ntasks
     variants = {"auto": gpm.TC_AUTO, "bitmap": gpm.TC_BITMAP, "hash": gpm.TC_HASH, "bsearch": gpm.TC_BSEARCH,
                 "merge": gpm.TC_MERGE, "learned": gpm.TC_LEARNED}
     variant = variants[args.variant]
@@ -456,10 +457,10 @@ def tc_line(args, rank, world, dist, local):
                                     "clipped, so it never reads these bytes"},
                     requested={"bytes": bytes_req, "gbs": bytes_req / (avg_kernel_ms / 1e3) / 1e9,
                                "frac": bytes_req / (avg_kernel_ms / 1e3) / 1e9 / hbm,
-                               "note": "bytes the kernel loads (segment keys and descriptors, owner lists), "
+                               "note": "bytes the kernel loads (segment keys, core-row words and descriptors, owner lists), "
                                        "mostly served by L2"},
                     plan={"segments": nseg, "segment_keys": seg_keys, "owner_keys": owner_keys,
-                          "owner_tasks": ntasks})
+                          "owner_tasks": ntasks, "dense_segments": dense_segs, "dense_words": dense_words})
     line = {
         "metric": METRIC,
         "value": value, "unit": "TEPS", "n_gpus": world, "steps": args.steps, "warmup": warm,
@@ -476,8 +477,9 @@ def tc_line(args, rank, world, dist, local):
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        # one count kernel per step (k_tc_rank, or k_tc_hash / k_tc_bsearch / k_tc_merge)
-        "gpu_launches": args.steps,
+        # per step one count kernel (k_tc_rank, or k_tc_hash / k_tc_bsearch / k_tc_merge), and k_tc_dense
+        # beside k_tc_rank when the plan has dense core segments
+        "gpu_launches": args.steps * (2 if dense_segs and args.variant in ("auto", "bitmap") else 1),
     }
     g.close()
     return line

@@ -174,7 +174,7 @@ __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restr
   long long mx = 0, nlong = 0;
   for (int i = (int)lane; i < nseg; i += 32) {
     const longlong2 sg = pseg[i < nl ? poff[x] + i : back + i];
-    long long len = sg.y - sg.x;
+    long long len = sg.x < 0 ? sg.y : sg.y - sg.x;  // a dense segment {-1 - row, keys}
     work += (unsigned long long)len;
     mx = max(mx, len);
     nlong += len >= 32;
@@ -275,16 +275,20 @@ __global__ void k_rail(const int32_t *__restrict__ tasks, int ntasks, const floa
 
 static int blocks(int64_t work) { return (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, num_sms() * 8)); }
 
-// all owners of the heuristic plan, in one device list
+// all owners of the heuristic plan, in one device list (the owners whose
+// segments are all dense, and so in neither of its queues, included)
 static int all_tasks(gpm_graph *g, DevBuf<int32_t> &tasks, int *ntasks, cudaStream_t st) {
   GPM_TRY(rank_build_plan(g, kRankCtaMin, kRankLongMin, st));
   RankPlan *p = g->rank;
-  *ntasks = p->n_cta + p->n_warp;
+  *ntasks = p->n_cta + p->n_warp + p->n_dense_only;
   GPM_TRY(tasks.reserve(std::max(1, *ntasks)));
   if (p->n_cta)
     GPM_CUDA(cudaMemcpyAsync(tasks.p, p->cta_tasks.p, sizeof(int32_t) * p->n_cta, cudaMemcpyDeviceToDevice, st));
   if (p->n_warp)
     GPM_CUDA(cudaMemcpyAsync(tasks.p + p->n_cta, p->warp_tasks.p, sizeof(int32_t) * p->n_warp,
+                             cudaMemcpyDeviceToDevice, st));
+  if (p->n_dense_only)
+    GPM_CUDA(cudaMemcpyAsync(tasks.p + p->n_cta + p->n_warp, p->dense_only.p, sizeof(int32_t) * p->n_dense_only,
                              cudaMemcpyDeviceToDevice, st));
   return GPM_OK;
 }

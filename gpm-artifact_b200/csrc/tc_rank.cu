@@ -20,6 +20,13 @@
 //    list spans few ids, so membership is one shared-memory byte load (span
 //    within the byte map) or bit test (within the bitmap): no hashing, no
 //    probe loops, no divergence.  Wider owners use an open-addressing table.
+// 5. Dense core.  The top 16,384 ranks are dense among themselves: an owner
+//    there meets partners whose clipped lists hold many keys per 32 ids of
+//    its span.  Such a partner's core keys are kept as a bitmap row, and the
+//    segment is counted as popc(row & N(owner)) over the owner's span by
+//    k_tc_dense (one 32-bit word per 32 ids instead of one key per id) on a
+//    side stream beside the count kernel (R-MAT 22: 4.2 G of the 8.15 G
+//    streamed keys become 1.7 G words).
 //
 // Long segments are streamed by half-warps, one coalesced row of 16 keys per
 // step; short ones by 8-lane groups.  Owners with more than `cta_min` keys
@@ -30,6 +37,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -92,6 +100,9 @@ struct HashTable {
 #ifndef GPM_RANK_SHORT_LANES
 #define GPM_RANK_SHORT_LANES 4  // lanes per short segment (2, 4, 8 or 16)
 #endif
+#ifndef GPM_RANK_BYTEMAP
+#define GPM_RANK_BYTEMAP 1  // 0: owners whose span fits a byte map use the bitmap
+#endif
 #ifndef GPM_RANK_UNROLL
 #define GPM_RANK_UNROLL 1
 #endif
@@ -109,6 +120,8 @@ __device__ __forceinline__ unsigned hit4(const T &t, int4 v) {
 // eight segments per warp at 4 lanes.
 // `wid`/`nw` spread segments over the warps of the executing group (1 warp
 // for warp tasks, the CTA's warps for CTA tasks).
+// Dense long segments ({-1 - i, keys}, owners in the dense core) are counted
+// by k_tc_dense and skipped here.
 template <class T>
 __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__restrict__ radj4,
                                                             const longlong2 *__restrict__ pseg, int64_t l0,
@@ -121,7 +134,7 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
   for (j = l0 + wid * 2 + half; j < l1; j += nw * 2) {
     const longlong2 sg = pseg[j];
     const int4 *__restrict__ q = rows + (sg.x >> 2);
-    const int nr = (int)(((sg.y + 3) >> 2) - (sg.x >> 2));
+    const int nr = sg.x < 0 ? 0 : (int)(((sg.y + 3) >> 2) - (sg.x >> 2));  // dense: none
     unsigned cs = 0;
 #pragma unroll kRankUnroll
     for (int i = (int)hl; i < nr; i += 16) cs += hit4(t, __ldg(q + i));
@@ -174,8 +187,8 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
   const int32_t kmin = radj[s0], kmax = radj[s0 + d - 1];
   const int64_t span = (int64_t)kmax - kmin + 1;
   unsigned long long c = 0;
-  // byte map / bitmap: span + 1 entries, the last the zero guard
-  if (span < (int64_t)nwords * 4) {
+  if (GPM_RANK_BYTEMAP && span < (int64_t)nwords * 4) {
+    // byte map / bitmap: span + 1 entries, the last the zero guard
     const int nclear = (int)((span + 4) >> 2);
     for (int i = tid; i < nclear; i += nthr) words[i] = 0u;
     group_sync<CTA>();
@@ -264,6 +277,65 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
   if (lane == 0 && c) atomicAdd(out, c);
 }
 #define k_tc_rank k_tc_rank_t<false>
+
+// Dense segments of the core owners, one owner per CTA task (heaviest
+// first): N(x) as a bitmap from base = min N(x) rounded down to 128 in shared
+// memory (core_clear_words, at most row_words + 4), then every dense long
+// segment {-1 - i, keys} of x by a group of kDenseLanes lanes: the partner's
+// core row words from base on (rows4[i] ..), ANDed 16 bytes per lane with the
+// bitmap over core_and_words(x) / 4 loads.  Its own launch, so that its
+// register budget (64 at 4 CTAs of 256 per SM) allows several 16-byte loads
+// in flight per lane; the owners' other segments run in k_tc_rank.
+constexpr int kDenseLanes = 8;
+#ifndef GPM_RANK_DENSE_UNROLL
+#define GPM_RANK_DENSE_UNROLL 4
+#endif
+constexpr int kDenseUnroll = GPM_RANK_DENSE_UNROLL;
+__global__ void __launch_bounds__(256, 4)
+    k_tc_dense(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
+               const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
+               const int32_t *__restrict__ tasks, int ntasks, const uint4 *__restrict__ rows4,
+               int *__restrict__ counter, unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) uint32_t dsm[];
+  __shared__ int s_task;
+  const int grp = threadIdx.x / kDenseLanes, gl = threadIdx.x % kDenseLanes, ngrp = blockDim.x / kDenseLanes;
+  const uint4 *b = reinterpret_cast<const uint4 *>(dsm);
+  unsigned long long c = 0;
+  while (true) {
+    if (threadIdx.x == 0) s_task = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = s_task;
+    __syncthreads();
+    if (t >= ntasks) break;
+    const int32_t x = tasks[t];
+    const int64_t s0 = roff[x], s1 = roff[x + 1];
+    const int32_t kmin = radj[s0], kmax = radj[s1 - 1], base = kmin & ~127;
+    const int nclear = core_clear_words(kmin, kmax), nq = core_and_words(kmin, kmax) >> 2;
+    for (int i = threadIdx.x; i < nclear; i += blockDim.x) dsm[i] = 0u;
+    __syncthreads();
+    for (int64_t k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
+      const uint32_t o = (uint32_t)(radj[k] - base);
+      atomicOr(&dsm[o >> 5], 1u << (o & 31));
+    }
+    __syncthreads();
+    const int64_t l0 = poff[x], l1 = l0 + plong[x];
+    for (int64_t j = l0 + grp; j < l1; j += ngrp) {
+      const int64_t sx = pseg[j].x;
+      if (sx >= 0) continue;
+      const uint4 *__restrict__ r = rows4 + (-1 - sx);
+      unsigned cs = 0;
+#pragma unroll kDenseUnroll
+      for (int i = gl; i < nq; i += kDenseLanes) {
+        const uint4 a = __ldg(r + i), m = b[i];
+        cs += __popc(a.x & m.x) + __popc(a.y & m.y) + __popc(a.z & m.z) + __popc(a.w & m.w);
+      }
+      c += cs;
+    }
+    __syncthreads();
+  }
+  c = warp_sum(c);
+  if (lane_id() == 0 && c) atomicAdd(out, c);
+}
 
 // ------------------------------------------------------------ plan build
 __global__ void k_indeg(int64_t nnz, const int32_t *__restrict__ adj, int32_t *__restrict__ indeg) {
@@ -436,7 +508,9 @@ __global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, con
                                 int long_min, const uint8_t *__restrict__ cfg,
                                 const int64_t *__restrict__ poff, int32_t *__restrict__ plong,
                                 int32_t *__restrict__ pshort, longlong2 *__restrict__ pseg,
-                                unsigned long long *__restrict__ work) {
+                                unsigned long long *__restrict__ work, int32_t core_base,
+                                const int32_t *__restrict__ rowid, int row_words, int dense_pct,
+                                int32_t *__restrict__ pdense) {
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = warp; u < n; u += nw) {
@@ -463,21 +537,63 @@ __global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, con
                                 : lower_bound_key(radj, ps, pe, radj[os]);
       const int64_t len = upper_bound_key(radj, lo, pe, radj[oe - 1]) - lo;
       if (len == 0) continue;
-      const bool lng = len >= owner_long_min(cfg, owner, long_min);
+      const int32_t partner = own_u ? v : (int32_t)u;
+      // dense: a core owner and a partner with a core row, the keys at least
+      // dense_pct % of the owner's words to AND (k_tc_dense counts it; the
+      // count kernel only skips its descriptor)
+      int64_t row = -1;  // dense: the uint4 index of the partner's row words from the owner's base
+      if (rowid && radj[os] >= core_base) {
+        const int32_t kmin = radj[os], r = rowid[partner];
+        if (r >= 0 && 100 * len >= (int64_t)dense_pct * core_and_words(kmin, radj[oe - 1]))
+          row = (int64_t)r * (row_words >> 2) + (((kmin & ~127) - core_base) >> 7);
+      }
+      const int64_t units = row >= 0 ? 0 : len;
+      const bool lng = row >= 0 || len >= owner_long_min(cfg, owner, long_min);
       cg::coalesced_group grp =
           cg::labeled_partition(cg::coalesced_threads(), ((unsigned long long)(uint32_t)owner << 1) | lng);
       int base = 0;
       if (grp.thread_rank() == 0) base = atomicAdd(lng ? &plong[owner] : &pshort[owner], (int)grp.size());
       const int64_t slot = grp.shfl(base, 0) + (int64_t)grp.thread_rank();
       const int64_t pos = lng ? poff[owner] + slot : poff[owner + 1] - 1 - slot;
-      const int32_t partner = own_u ? v : (int32_t)u;
       const int64_t lo4 = lo - roff[partner] + roff4[partner];  // the same keys in radj4
-      pseg[pos] = make_longlong2(lo4, lo4 + len);
-      const unsigned long long w = cg::reduce(grp, (unsigned long long)len + 1ull, cg::plus<unsigned long long>());
+      pseg[pos] = row >= 0 ? make_longlong2(-1 - row, len) : make_longlong2(lo4, lo4 + len);
+      const unsigned long long w = cg::reduce(grp, (unsigned long long)units + 1ull, cg::plus<unsigned long long>());
       if (grp.thread_rank() == 0) atomicAdd(&work[owner], w);
+      if (rowid) {
+        const int nd = __popc(grp.ballot(row >= 0));
+        if (nd && grp.thread_rank() == 0) atomicAdd(&pdense[owner], nd);
+      }
     }
   }
 }
+// Dense core rows: rowid[v] = a row number when v has at least min_keys
+// keys >= core_base, else -1 (*nrows counts the rows)
+__global__ void k_core_rowid(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+                             int32_t core_base, int min_keys, int32_t *__restrict__ rowid, int *__restrict__ nrows) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = roff[v + 1];
+    rowid[v] = e - lower_bound_key(radj, roff[v], e, core_base) >= min_keys ? atomicAdd(nrows, 1) : -1;
+  }
+}
+// row rowid[v] = v's keys >= core_base as bits from core_base (one warp per
+// vertex; rows zeroed first)
+__global__ void k_core_rows(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+                            int32_t core_base, const int32_t *__restrict__ rowid, int row_words,
+                            uint32_t *__restrict__ rows) {
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = warp; v < n; v += nw) {
+    const int32_t r = rowid[v];
+    if (r < 0) continue;
+    uint32_t *row = rows + (int64_t)r * row_words;
+    const int64_t e = roff[v + 1];
+    for (int64_t k = lower_bound_key(radj, roff[v], e, core_base) + lane_id(); k < e; k += 32) {
+      const uint32_t o = (uint32_t)(radj[k] - core_base);
+      atomicOr(&row[o >> 5], 1u << (o & 31));
+    }
+  }
+}
+
 // roff4: list lengths rounded up to a multiple of four, for the scan that
 // places every list of radj4 at a multiple of four keys
 __global__ void k_padded_len(int64_t n, const int64_t *__restrict__ roff, int64_t *__restrict__ len4) {
@@ -485,15 +601,32 @@ __global__ void k_padded_len(int64_t n, const int64_t *__restrict__ roff, int64_
     len4[v] = (roff[v + 1] - roff[v] + 3) & ~(int64_t)3;
 }
 
+// dense tasks: owners with dense segments, key = ~(their words to AND)
+__global__ void k_dense_tasks(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
+                              const int32_t *__restrict__ pdense, unsigned long long *__restrict__ key,
+                              int32_t *__restrict__ val, int *__restrict__ size) {
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+    if (pdense[x] == 0) continue;
+    const int i = atomicAdd(size, 1);
+    key[i] = ~((unsigned long long)pdense[x] * (unsigned long long)core_and_words(radj[roff[x]], radj[roff[x + 1] - 1]));
+    val[i] = (int32_t)x;
+  }
+}
+
 // tasks: owners with partners; key = ~work so an ascending sort puts heavy first
 __global__ void k_rank_tasks(int64_t n, const int64_t *__restrict__ roff, const int32_t *__restrict__ plong,
                              const int32_t *__restrict__ pshort,
                              const unsigned long long *__restrict__ work, int cta_min,
-                             const uint8_t *__restrict__ cfg, unsigned long long *__restrict__ ckey,
+                             const uint8_t *__restrict__ cfg, const int32_t *__restrict__ pdense,
+                             int32_t *__restrict__ donly, unsigned long long *__restrict__ ckey,
                              int32_t *__restrict__ cval, unsigned long long *__restrict__ wkey,
                              int32_t *__restrict__ wval, int *__restrict__ sizes) {
   for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
-    if (plong[x] + pshort[x] == 0) continue;
+    const int nd = pdense ? pdense[x] : 0;
+    if (plong[x] + pshort[x] == nd) {  // nothing left to stream
+      if (nd) donly[atomicAdd(&sizes[3], 1)] = (int32_t)x;  // dense segments only
+      continue;
+    }
     int64_t d = roff[x + 1] - roff[x];
     if (cfg ? cfg[x] / 3 == 1 : d > cta_min) {
       int i = atomicAdd(&sizes[0], 1);
@@ -904,6 +1037,51 @@ static int ensure_padded_lists(gpm_graph *g, cudaStream_t st, bool *fill) {
   return GPM_OK;
 }
 
+static int64_t env_or(const char *name, int64_t dflt) {
+  const char *e = getenv(name);
+  return e && *e ? atoll(e) : dflt;
+}
+
+// The dense core of a fixed plan: core_base, the rows and rowid (see
+// RankPlan).  GPM_TC_CORE, GPM_TC_CORE_MIN and GPM_TC_DENSE_PCT override
+// GPM_RANK_CORE, GPM_RANK_CORE_MIN and GPM_RANK_DENSE_PCT.  The rows are left
+// out (p->n_rows = 0) when none qualifies or they would take more than an
+// eighth of the free device memory.
+static int build_core_rows(gpm_graph *g, RankPlan *p, DevBuf<int32_t> &rowid, int *dense_pct, cudaStream_t st) {
+  const int64_t n = g->n;
+  const int64_t K = env_or("GPM_TC_CORE", GPM_RANK_CORE);
+  const int64_t min_keys = std::max<int64_t>(1, env_or("GPM_TC_CORE_MIN", GPM_RANK_CORE_MIN));
+  *dense_pct = (int)std::max<int64_t>(0, env_or("GPM_TC_DENSE_PCT", GPM_RANK_DENSE_PCT));
+  if (K <= 0 || n <= 0 || n > INT32_MAX - 128) return GPM_OK;
+  const int32_t core_base = (int32_t)(std::max<int64_t>(0, n - K) & ~(int64_t)127);
+  const int64_t row_words = ((n - core_base + 127) >> 7) << 2;
+  if (row_words > (int64_t)kRankCtaWords) return GPM_OK;  // wider than any owner bitmap
+  DevBuf<int> nrows;
+  GPM_TRY(rowid.reserve(n));
+  GPM_TRY(nrows.reserve(1));
+  GPM_CUDA(cudaMemsetAsync(nrows.p, 0, sizeof(int), st));
+  k_core_rowid<<<grid_for(n), 256, 0, st>>>(n, g->rg->roff.p, g->rg->radj.p, core_base, (int)min_keys, rowid.p,
+                                            nrows.p);
+  GPM_LAUNCH_CHECK();
+  int h = 0;
+  GPM_CUDA(cudaMemcpyAsync(&h, nrows.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GPM_CUDA(cudaStreamSynchronize(st));
+  if (h <= 0) return GPM_OK;
+  size_t free_b = 0, total_b = 0;
+  GPM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const size_t bytes = (size_t)h * (size_t)row_words * 4;
+  if (bytes > free_b / 8) return GPM_OK;
+  GPM_TRY(p->rows.reserve((size_t)h * (size_t)row_words));
+  GPM_CUDA(cudaMemsetAsync(p->rows.p, 0, bytes, st));
+  k_core_rows<<<grid_for(n * 32), 256, 0, st>>>(n, g->rg->roff.p, g->rg->radj.p, core_base, rowid.p,
+                                                (int)row_words, p->rows.p);
+  GPM_LAUNCH_CHECK();
+  p->core_base = core_base;
+  p->row_words = (int)row_words;
+  p->n_rows = h;
+  return GPM_OK;
+}
+
 int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, cudaStream_t st, RankPlan **out) {
   GPM_TRY(ensure_rank_graph(g, st));
   bool fill = false;
@@ -930,30 +1108,61 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
   cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(p->pshort.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
+  DevBuf<int32_t> rowid;
+  int dense_pct = 0;
+  if (!cfg) GPM_TRY(build_core_rows(g, p, rowid, &dense_pct, st));
+  if (p->n_rows) {
+    GPM_TRY(p->pdense.reserve(n));
+    GPM_CUDA(cudaMemsetAsync(p->pdense.p, 0, sizeof(int32_t) * n, st));
+  }
   k_partner_place<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, g->rg->roff4.p, fill ? g->rg->radj4.p : nullptr,
                                                      g->rg->upward, long_min, cfg, p->poff.p, p->plong.p, p->pshort.p,
-                                                     p->pseg.p, work.p);
+                                                     p->pseg.p, work.p, p->core_base, p->n_rows ? rowid.p : nullptr,
+                                                     p->row_words, dense_pct, p->pdense.p);
   GPM_LAUNCH_CHECK();
   if (fill) g->rg->padded = 1;
   // 3. task queues, heaviest first
   DevBuf<unsigned long long> ckey, wkey;
   DevBuf<int32_t> cval, wval;
+  DevBuf<unsigned long long> dkey;
+  DevBuf<int32_t> dval;
   DevBuf<int> sizes;
   if ((s = ckey.reserve(n)) || (s = wkey.reserve(n)) || (s = cval.reserve(n)) || (s = wval.reserve(n)) ||
-      (s = sizes.reserve(2)) || (s = p->cta_tasks.reserve(n)) || (s = p->warp_tasks.reserve(n)))
+      (s = sizes.reserve(4)) || (s = p->cta_tasks.reserve(n)) || (s = p->warp_tasks.reserve(n)))
     return bail(s);
-  cudaMemsetAsync(sizes.p, 0, 2 * sizeof(int), st);
-  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->plong.p, p->pshort.p, work.p, cta_min, cfg, ckey.p, cval.p,
-                                            wkey.p,
-                                            wval.p, sizes.p);
-  int h[2] = {0, 0};
+  cudaMemsetAsync(sizes.p, 0, 4 * sizeof(int), st);
+  const int32_t *pdense = p->n_rows ? p->pdense.p : nullptr;
+  if (pdense && (s = p->dense_only.reserve(n))) return bail(s);
+  k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->plong.p, p->pshort.p, work.p, cta_min, cfg, pdense,
+                                            p->dense_only.p, ckey.p, cval.p, wkey.p, wval.p, sizes.p);
+  if (pdense) {
+    if ((s = dkey.reserve(n)) || (s = dval.reserve(n))) return bail(s);
+    k_dense_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, radj, pdense, dkey.p, dval.p, sizes.p + 2);
+  }
+  int h[4] = {0, 0, 0, 0};
   cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank plan: ") + cudaGetErrorString(e)));
   p->n_cta = h[0];
   p->n_warp = h[1];
-  if ((s = sort_pairs_u64(ckey, cval, h[0], p->cta_tasks, st)) || (s = sort_pairs_u64(wkey, wval, h[1], p->warp_tasks, st)))
+  p->n_dense = h[2];
+  p->n_dense_only = h[3];
+  if (p->n_dense && (s = p->dense_tasks.reserve(p->n_dense))) return bail(s);
+  if ((s = sort_pairs_u64(ckey, cval, h[0], p->cta_tasks, st)) || (s = sort_pairs_u64(wkey, wval, h[1], p->warp_tasks, st)) ||
+      (s = sort_pairs_u64(dkey, dval, h[2], p->dense_tasks, st)))
     return bail(s);
+  if (p->n_dense) {
+    p->dense_smem = (size_t)(p->row_words + 4) * sizeof(uint32_t);
+    int per_sm = 0;
+    GPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_dense, 256, p->dense_smem));
+    p->dense_grid = std::max(1, std::min(per_sm * num_sms(), p->n_dense));
+    if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return bail(fail(GPM_ECUDA, "rank plan: stream or event for the dense kernel"));
+    }
+  }
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank plan: ") + cudaGetErrorString(e)));
   *out = p;
@@ -975,18 +1184,26 @@ int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long l
   GPM_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
   if (g->nnz == 0) return GPM_OK;
   GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 4 * sizeof(int), st));
+  if (p->n_dense) {  // forked onto the plan's side stream, joined after the count kernel
+    GPM_CUDA(cudaEventRecord(p->fork, st));
+    GPM_CUDA(cudaStreamWaitEvent(p->side, p->fork, 0));
+    k_tc_dense<<<p->dense_grid, 256, p->dense_smem, p->side>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p,
+                                                                p->plong.p, p->dense_tasks.p, p->n_dense,
+                                                                reinterpret_cast<const uint4 *>(p->rows.p),
+                                                                p->counters.p + 2, d_out);
+    GPM_LAUNCH_CHECK();
+    GPM_CUDA(cudaEventRecord(p->join, p->side));
+  }
   if (rec)
-    k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, g->rg->radj4.p,
-                                                           p->poff.p, p->pseg.p,
-                                                           p->plong.p, p->pshort.p, p->cta_tasks.p, p->n_cta, p->warp_tasks.p,
-                                                           p->n_warp, p->counters.p, d_out, rec);
+    k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(
+        g->rg->roff.p, g->rg->radj.p, g->rg->radj4.p, p->poff.p, p->pseg.p, p->plong.p, p->pshort.p, p->cta_tasks.p,
+        p->n_cta, p->warp_tasks.p, p->n_warp, p->counters.p, d_out, rec);
   else
     k_tc_rank<<<rank_grid(), 256, kRankSmem, st>>>(g->rg->roff.p, g->rg->radj.p, g->rg->radj4.p, p->poff.p,
-                                                   p->pseg.p, p->plong.p,
-                                                   p->pshort.p,
-                                                   p->cta_tasks.p, p->n_cta, p->warp_tasks.p, p->n_warp,
-                                                   p->counters.p, d_out, nullptr);
+                                                   p->pseg.p, p->plong.p, p->pshort.p, p->cta_tasks.p, p->n_cta,
+                                                   p->warp_tasks.p, p->n_warp, p->counters.p, d_out, nullptr);
   GPM_LAUNCH_CHECK();
+  if (p->n_dense) GPM_CUDA(cudaStreamWaitEvent(st, p->join, 0));
   return GPM_OK;
 }
 
@@ -1002,46 +1219,62 @@ int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
 __global__ void k_plan_stats(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
                              const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
                              const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
-                             unsigned long long *__restrict__ out) {
-  unsigned long long segs = 0, keys = 0, okeys = 0;
+                             const int32_t *__restrict__ radj, unsigned long long *__restrict__ out) {
+  unsigned long long segs = 0, keys = 0, okeys = 0, dsegs = 0, dwords = 0;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntasks; t += (int64_t)gridDim.x * blockDim.x) {
     const int32_t x = tasks[t];
     okeys += (unsigned long long)(roff[x + 1] - roff[x]);
     segs += (unsigned long long)(plong[x] + pshort[x]);
-    for (int64_t j = poff[x]; j < poff[x] + plong[x]; ++j) keys += (unsigned long long)(pseg[j].y - pseg[j].x);
+    for (int64_t j = poff[x]; j < poff[x] + plong[x]; ++j) {
+      if (pseg[j].x < 0) {  // dense: the owner's bitmap words
+        ++dsegs;
+        dwords += (unsigned long long)core_and_words(radj[roff[x]], radj[roff[x + 1] - 1]);
+      } else {
+        keys += (unsigned long long)(pseg[j].y - pseg[j].x);
+      }
+    }
     for (int64_t j = poff[x + 1] - pshort[x]; j < poff[x + 1]; ++j)
       keys += (unsigned long long)(pseg[j].y - pseg[j].x);
   }
   segs = warp_sum(segs);
   keys = warp_sum(keys);
   okeys = warp_sum(okeys);
+  dsegs = warp_sum(dsegs);
+  dwords = warp_sum(dwords);
   if (lane_id() == 0) {
     atomicAdd(&out[0], segs);
     atomicAdd(&out[1], keys);
     atomicAdd(&out[2], okeys);
+    atomicAdd(&out[3], dsegs);
+    atomicAdd(&out[4], dwords);
   }
 }
 
 int rank_plan_stats(gpm_graph *g, uint64_t *out) {
-  out[0] = out[1] = out[2] = out[3] = 0;
+  for (int i = 0; i < 6; ++i) out[i] = 0;
   if (g->nnz == 0) return GPM_OK;
   GPM_TRY(rank_build_plan(g, kRankCtaMin, kRankLongMin, 0));
   RankPlan *p = g->rank;
   DevBuf<unsigned long long> o;
-  GPM_TRY(o.reserve(3));
-  GPM_CUDA(cudaMemset(o.p, 0, 24));
+  GPM_TRY(o.reserve(5));
+  GPM_CUDA(cudaMemset(o.p, 0, 40));
   const int grid = num_sms() * 8;
   k_plan_stats<<<grid, 256>>>(p->cta_tasks.p, p->n_cta, g->rg->roff.p, p->poff.p, p->pseg.p, p->plong.p,
-                              p->pshort.p, o.p);
+                              p->pshort.p, g->rg->radj.p, o.p);
   k_plan_stats<<<grid, 256>>>(p->warp_tasks.p, p->n_warp, g->rg->roff.p, p->poff.p, p->pseg.p, p->plong.p,
-                              p->pshort.p, o.p);
+                              p->pshort.p, g->rg->radj.p, o.p);
+  if (p->n_dense_only)
+    k_plan_stats<<<grid, 256>>>(p->dense_only.p, p->n_dense_only, g->rg->roff.p, p->poff.p, p->pseg.p, p->plong.p,
+                                p->pshort.p, g->rg->radj.p, o.p);
   GPM_LAUNCH_CHECK();
-  unsigned long long h[3];
+  unsigned long long h[5];
   GPM_CUDA(cudaMemcpy(h, o.p, sizeof h, cudaMemcpyDeviceToHost));
   out[0] = h[0];
   out[1] = h[1];
   out[2] = h[2];
-  out[3] = (uint64_t)(p->n_cta + p->n_warp);
+  out[3] = (uint64_t)(p->n_cta + p->n_warp + p->n_dense_only);
+  out[4] = h[3];
+  out[5] = h[4];
   return GPM_OK;
 }
 

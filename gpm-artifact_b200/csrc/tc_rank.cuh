@@ -54,6 +54,35 @@ struct RankGraph {
   int padded = 0;  // radj4 written
 };
 
+#ifndef GPM_RANK_CORE
+// dense core of the fixed plan: the top this-many ranks (0: none).  R-MAT 22
+// holds 64 % of its streamed keys in owners of the top 16,384 ranks
+#define GPM_RANK_CORE 16384
+#endif
+#ifndef GPM_RANK_CORE_MIN
+// a vertex gets a core bitmap row when at least this many of its keys lie
+// in the core (R-MAT 22: 86,115 rows of 2 KB)
+#define GPM_RANK_CORE_MIN 128
+#endif
+#ifndef GPM_RANK_DENSE_PCT
+// a core owner's segment with a row is ANDed as bitmap words when its key
+// count is at least this percentage of the words to AND
+#define GPM_RANK_DENSE_PCT 100
+#endif
+
+// Core bitmaps of an owner x whose keys all lie in the core (min N(x) >=
+// core_base): N(x) as bits from base = min N(x) rounded down to 128, so
+// bitmap word i lines up with word (base - core_base) / 32 + i of every core
+// row and 16-byte loads of both stay aligned.  and_words: the words that can
+// hold keys of N(x) (a multiple of four); clear_words: those plus the word of
+// the zero guard bit at max N(x) - base + 1 (a multiple of four).
+__host__ __device__ __forceinline__ int core_and_words(int32_t kmin, int32_t kmax) {
+  return (((kmax - (kmin & ~127)) >> 5) + 4) & ~3;
+}
+__host__ __device__ __forceinline__ int core_clear_words(int32_t kmin, int32_t kmax) {
+  return (((kmax - (kmin & ~127) + 1) >> 5) + 4) & ~3;
+}
+
 // Per-graph schedule of GPM_TC_BITMAP (device arrays):
 //   poff/pseg   partner segments: owner x has the room pseg[poff[x] ..
 //               poff[x+1]) (poff = rinc, one slot per incident edge); its
@@ -63,9 +92,40 @@ struct RankGraph {
 //               partner's list inside [min N(x), max N(x)] (no key outside
 //               that range can be in N(x)); empty ranges are left out
 //   cta_tasks / warp_tasks  owners by size class, heaviest first
+//   rows        dense core (fixed plan only): ranks [core_base, n) with
+//               core_base a multiple of 128; row r holds, as row_words bits
+//               from core_base, the core keys of one vertex that has at
+//               least GPM_RANK_CORE_MIN of them.  A long segment
+//               {-1 - i, keys} is dense: its owner lies in the core and the
+//               count is popc(row & N(owner)) over the owner's words, with
+//               the partner's row words from the owner's base on starting at
+//               uint4 index i of rows, instead of streaming the partner's
+//               keys; k_tc_dense counts these (tasks: dense_tasks) and the
+//               count kernel skips them
 struct RankPlan {
   int cta_min = 0, long_min = 0;
   int n_cta = 0, n_warp = 0;
+  int32_t core_base = INT32_MAX;  // INT32_MAX: no dense core
+  int row_words = 0;              // multiple of 4
+  int64_t n_rows = 0;
+  DevBuf<uint32_t> rows;
+  DevBuf<int32_t> pdense;       // dense segments per owner
+  DevBuf<int32_t> dense_tasks;  // owners with dense segments, most words first
+  DevBuf<int32_t> dense_only;   // owners with dense segments only (in neither task queue)
+  int n_dense = 0, n_dense_only = 0, dense_grid = 0;
+  size_t dense_smem = 0;
+  // k_tc_dense runs on `side`, forked from and joined back into the caller's
+  // stream by the two events, so that it overlaps the count kernel
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  RankPlan() = default;
+  RankPlan(const RankPlan &) = delete;
+  RankPlan &operator=(const RankPlan &) = delete;
+  ~RankPlan() {
+    if (side) cudaStreamSynchronize(side), cudaStreamDestroy(side);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+  }
   DevBuf<int64_t> poff;
   DevBuf<longlong2> pseg;
   DevBuf<int32_t> plong, pshort;
@@ -85,7 +145,8 @@ int ensure_rank_graph(gpm_graph *g, cudaStream_t st, const int32_t *gid = nullpt
 int build_upward_rank_graph(gpm_graph *g, cudaStream_t st, const int64_t *h_off, const int32_t *h_adj);
 int rank_build_plan(gpm_graph *g, int cta_min, int long_min, cudaStream_t st);
 int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out);
-// out[0..3]: segments, keys in them, owner-list keys, owner tasks of the fixed plan
+// out[0..5]: segments, keys streamed from the key segments, owner-list keys,
+// owner tasks, dense segments, bitmap words ANDed for them (fixed plan)
 int rank_plan_stats(gpm_graph *g, uint64_t *out);
 // An uncached plan; cfg (device, one byte per vertex, may be nullptr) gives
 // each owner its queue (cfg / 3: 0 warp, 1 CTA) and long-segment threshold

@@ -311,9 +311,9 @@ class Graph:
         return w.value, p.value
 
     def plan_stats(self):
-        """(segments, streamed keys, owner keys, owner tasks) of the fixed
-        GPM_TC_BITMAP plan."""
-        st = np.zeros(4, np.uint64)
+        """(segments, streamed keys, owner keys, owner tasks, dense segments,
+        bitmap words ANDed for them) of the fixed GPM_TC_BITMAP plan."""
+        st = np.zeros(6, np.uint64)
         check(lib.gpm_tc_plan_stats(self.h, _ptr(st)))
         return tuple(int(x) for x in st)
 

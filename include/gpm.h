@@ -195,9 +195,11 @@ int gpm_tc_async(gpm_graph *g, int variant, void *stream, uint64_t *d_out);
 int gpm_tc_host_csr(int64_t n, const int64_t *offsets, const int32_t *indices, int variant,
                     void *stream, uint64_t *out);
 /* Work of GPM_TC_BITMAP's fixed plan on g (built if needed), no reference
- * counterpart: stats[0] partner segments, stats[1] keys streamed from them,
- * stats[2] keys of the owner lists loaded into shared memory, stats[3] owner
- * tasks. */
+ * counterpart: stats[0] partner segments, stats[1] keys streamed from the
+ * segments read as keys, stats[2] keys of the owner lists loaded into shared
+ * memory, stats[3] owner tasks, stats[4] dense segments (read as 32-bit
+ * words of a core bitmap row), stats[5] the words ANDed for them.  stats
+ * holds 6 entries. */
 int gpm_tc_plan_stats(gpm_graph *g, uint64_t *stats);
 
 /* Triangle count of a device-resident CSR that allocates nothing -- this

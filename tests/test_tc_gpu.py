@@ -122,11 +122,25 @@ def test_host_csr_end_to_end():
         assert gpm.tc_host_csr(off, idx, v) == want
 
 
-def plan_numpy(off, idx):
+def core_words(kmin, kmax):
+    """(and_words, clear_words) of a core owner's bitmap based at kmin
+    rounded down to 128 (multiples of four words)."""
+    base = kmin & ~127
+    return (((kmax - base) >> 5) + 4) & ~3, (((kmax - base + 1) >> 5) + 4) & ~3
+
+
+def plan_numpy(off, idx, core=16384, core_min=128, dense_pct=100, cta_min=50, cta_words=6144):
     """The fixed plan's work restated in numpy: rank by (degree, id), DAG
     edges upward, owner = endpoint with the longer out-list (ties to the
     source), segment = the partner's list clipped to [min, max] of the
-    owner's list (owners with fewer than 2 keys have none)."""
+    owner's list (owners with fewer than 2 keys have none).  Dense core:
+    ranks from core_base = (n - core) rounded down to 128; a vertex with at
+    least core_min keys there has a row; a segment is dense when its owner's
+    keys all lie in the core, its owner's core bitmap fits the owner's queue
+    (cta_words, an eighth for warp tasks), its partner has a row and its keys
+    are at least dense_pct % of the owner's bitmap words.  Returns (segments,
+    keys of the non-dense segments, owner keys, owner tasks, dense segments,
+    their words)."""
     n = len(off) - 1
     deg = np.diff(off)
     order = np.lexsort((np.arange(n), deg))
@@ -151,7 +165,18 @@ def plan_numpy(off, idx):
     clip = np.where(np.maximum(du, dv) >= 2, np.maximum(b - a, 0), 0)
     seg = clip > 0
     tasks = np.unique(owner[seg])
-    return int(seg.sum()), int(clip.sum()), int(dp[tasks].sum()), len(tasks)
+    dense = np.zeros_like(seg)
+    aw = np.zeros(len(seg), np.int64)
+    cb = max(0, n - core) & ~127
+    row_words = ((n - cb + 127) >> 7) << 2
+    rowed = np.bincount(us[vs >= cb], minlength=n) >= max(1, core_min)
+    if core > 0 and n > 0 and row_words <= cta_words and rowed.any():
+        ko, kx = kmin[owner].astype(np.int64), kmax[owner].astype(np.int64)
+        aw, cw = core_words(ko, kx)
+        nwords = np.where(dp[owner] > cta_min, cta_words, cta_words // 8)
+        dense = seg & (ko >= cb) & rowed[partner] & (cw <= nwords) & (100 * clip >= dense_pct * aw)
+    return (int(seg.sum()), int(clip[~dense].sum()), int(dp[tasks].sum()), len(tasks), int(dense.sum()),
+            int(aw[dense].sum()))
 
 
 @pytest.mark.parametrize("kind", ["rmat", "er"])
@@ -165,6 +190,38 @@ def test_plan_segments_match_numpy(kind):
     off, idx = orc.build_csr(n, s, d)
     g = gpm.Graph.from_csr(off, idx).orient()
     assert g.plan_stats() == plan_numpy(off, idx)
+
+
+@pytest.mark.parametrize("case", [("rmat", 4096, 2, 0), ("rmat", 1 << 20, 1, 0), ("rmat", 8192, 16, 50),
+                                  ("er", 1 << 20, 1, 0), ("clique", 16384, 128, 100)])
+def test_dense_core_rows(case, monkeypatch):
+    """Dense core segments (core bitmap rows ANDed with the owner's bitmap)
+    count the same triangles: the thresholds lowered so that most segments of
+    core owners are dense, on R-MAT, Erdos-Renyi and a graph with a
+    1200-clique; the plan's dense segments and words equal the numpy
+    restatement."""
+    kind, core, core_min, pct = case
+    monkeypatch.setenv("GPM_TC_CORE", str(core))
+    monkeypatch.setenv("GPM_TC_CORE_MIN", str(core_min))
+    monkeypatch.setenv("GPM_TC_DENSE_PCT", str(pct))
+    if kind == "rmat":
+        n, s, d = gpm.gen_rmat(14, 16, seed=5)
+    elif kind == "er":
+        n, s, d = gpm.gen_er(6000, 400000, seed=5)
+    else:
+        n = 5000
+        iu, ju = np.triu_indices(1200, 1)
+        fr = np.random.default_rng(4).integers(0, n, size=(20000, 2))
+        s = np.concatenate([iu, fr[:, 0]]).astype(np.int32)
+        d = np.concatenate([ju, fr[:, 1]]).astype(np.int32)
+    off, idx, doff, didx = oracle_graph(n, s, d)
+    want = orc.tc(doff, didx)
+    g = gpm.Graph.from_edges(n, s, d).orient()
+    stats = g.plan_stats()
+    assert stats == plan_numpy(off, idx, core, core_min, pct)
+    assert stats[4] > 0
+    assert tc_all_variants(g) == [want] * len(VARIANTS)
+    assert gpm.tc_host_csr(off, idx, gpm.TC_AUTO) == want
 
 
 def test_lists_longer_than_the_sort_buffer():
