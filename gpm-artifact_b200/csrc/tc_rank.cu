@@ -28,16 +28,18 @@
 //    side stream beside the count kernel (R-MAT 22: 4.2 G of the 8.15 G
 //    streamed keys become 1.7 G words).
 //
-// Long segments are streamed by half-warps, one coalesced row of 16 keys per
-// step; short ones by 8-lane groups.  Owners with more than `cta_min` keys
-// are CTA tasks, the rest warp tasks; both queues are sorted heaviest first
-// and drained by a persistent grid.
+// Long segments (48 keys or more in the fixed schedule) are streamed by
+// half-warps, one coalesced 256-byte row of 64 keys per step; short ones by
+// 4-lane groups.  Owners with more than `cta_min` keys are CTA tasks, the
+// rest warp tasks; both queues are sorted heaviest first and drained by a
+// persistent grid.
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -286,9 +288,17 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
 // bitmap over core_and_words(x) / 4 loads.  Its own launch, so that its
 // register budget (64 at 4 CTAs of 256 per SM) allows several 16-byte loads
 // in flight per lane; the owners' other segments run in k_tc_rank.
-constexpr int kDenseLanes = 8;
+#ifndef GPM_RANK_DENSE_LANES
+// lanes per dense segment: 8 (R-MAT 22 5.88 ms at unroll 2) against 4 (5.79)
+// and 16 (6.27); 8 kept with unroll 1 (5.50 against 5.69 at 4 lanes)
+#define GPM_RANK_DENSE_LANES 8
+#endif
+constexpr int kDenseLanes = GPM_RANK_DENSE_LANES;
 #ifndef GPM_RANK_DENSE_UNROLL
-#define GPM_RANK_DENSE_UNROLL 4
+// 16-byte loads unrolled per lane: 1 (28 registers) ran R-MAT 22 in 5.78 ms
+// against 5.88 at 2 (40 registers) and 6.16 at 4 (56 registers): the kernel
+// shares the SMs with the count kernel, and fewer registers leave it more room
+#define GPM_RANK_DENSE_UNROLL 1
 #endif
 constexpr int kDenseUnroll = GPM_RANK_DENSE_UNROLL;
 __global__ void __launch_bounds__(256, 4)
@@ -1037,16 +1047,49 @@ static int ensure_padded_lists(gpm_graph *g, cudaStream_t st, bool *fill) {
   return GPM_OK;
 }
 
+// Resident CTAs of k_tc_dense x SMs (its largest shared-memory size, rows
+// of kRankCtaWords words, does not limit its occupancy).
+static int dense_grid() {
+  static PerDevice grid;
+  return grid.get([] {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_dense, 256, (kRankCtaWords + 4) * sizeof(uint32_t));
+    return std::max(1, per_sm) * num_sms();
+  });
+}
+
+// The side stream of the current device that k_tc_dense runs on (created on
+// first use, kept until the process exits; every plan of the device shares it).
+static cudaStream_t dense_stream(int *status) {
+  static std::mutex mu;
+  static cudaStream_t side[64];
+  int dev = 0;
+  *status = GPM_OK;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    *status = fail(GPM_ECUDA, "dense kernel: no current device below index 64");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!side[dev] && cudaStreamCreateWithFlags(&side[dev], cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    side[dev] = nullptr;
+    *status = fail(GPM_ECUDA, "dense kernel: side stream");
+  }
+  return side[dev];
+}
+
 static int64_t env_or(const char *name, int64_t dflt) {
   const char *e = getenv(name);
   return e && *e ? atoll(e) : dflt;
 }
 
-// The dense core of a fixed plan: core_base, the rows and rowid (see
+// The dense core of a plan: core_base, the rows and rowid (see
 // RankPlan).  GPM_TC_CORE, GPM_TC_CORE_MIN and GPM_TC_DENSE_PCT override
 // GPM_RANK_CORE, GPM_RANK_CORE_MIN and GPM_RANK_DENSE_PCT.  The rows are left
-// out (p->n_rows = 0) when none qualifies or they would take more than an
-// eighth of the free device memory.
+// out (p->n_rows = 0) when none qualifies or they would take more than 1 GiB
+// and more than four times the bytes of the rank graph's lists (R-MAT 22:
+// 176 MB of rows against 257 MB of lists).
 static int build_core_rows(gpm_graph *g, RankPlan *p, DevBuf<int32_t> &rowid, int *dense_pct, cudaStream_t st) {
   const int64_t n = g->n;
   const int64_t K = env_or("GPM_TC_CORE", GPM_RANK_CORE);
@@ -1067,10 +1110,8 @@ static int build_core_rows(gpm_graph *g, RankPlan *p, DevBuf<int32_t> &rowid, in
   GPM_CUDA(cudaMemcpyAsync(&h, nrows.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   GPM_CUDA(cudaStreamSynchronize(st));
   if (h <= 0) return GPM_OK;
-  size_t free_b = 0, total_b = 0;
-  GPM_CUDA(cudaMemGetInfo(&free_b, &total_b));
   const size_t bytes = (size_t)h * (size_t)row_words * 4;
-  if (bytes > free_b / 8) return GPM_OK;
+  if (bytes > std::max<size_t>((size_t)1 << 30, 16 * (size_t)g->rg->radj.n)) return GPM_OK;
   GPM_TRY(p->rows.reserve((size_t)h * (size_t)row_words));
   GPM_CUDA(cudaMemsetAsync(p->rows.p, 0, bytes, st));
   k_core_rows<<<grid_for(n * 32), 256, 0, st>>>(n, g->rg->roff.p, g->rg->radj.p, core_base, rowid.p,
@@ -1110,7 +1151,8 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
   DevBuf<int32_t> rowid;
   int dense_pct = 0;
-  if (!cfg) GPM_TRY(build_core_rows(g, p, rowid, &dense_pct, st));
+  // the dense core does not depend on the schedule: every plan has it
+  GPM_TRY(build_core_rows(g, p, rowid, &dense_pct, st));
   if (p->n_rows) {
     GPM_TRY(p->pdense.reserve(n));
     GPM_CUDA(cudaMemsetAsync(p->pdense.p, 0, sizeof(int32_t) * n, st));
@@ -1153,14 +1195,11 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
     return bail(s);
   if (p->n_dense) {
     p->dense_smem = (size_t)(p->row_words + 4) * sizeof(uint32_t);
-    int per_sm = 0;
-    GPM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_dense, 256, p->dense_smem));
-    p->dense_grid = std::max(1, std::min(per_sm * num_sms(), p->n_dense));
-    if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
+    p->dense_grid = std::max(1, std::min(dense_grid(), p->n_dense));
+    if (cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
-      return bail(fail(GPM_ECUDA, "rank plan: stream or event for the dense kernel"));
+      return bail(fail(GPM_ECUDA, "rank plan: events for the dense kernel"));
     }
   }
   e = cudaStreamSynchronize(st);
@@ -1184,15 +1223,18 @@ int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long l
   GPM_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
   if (g->nnz == 0) return GPM_OK;
   GPM_CUDA(cudaMemsetAsync(p->counters.p, 0, 4 * sizeof(int), st));
-  if (p->n_dense) {  // forked onto the plan's side stream, joined after the count kernel
+  if (p->n_dense) {  // forked onto the device's side stream, joined after the count kernel
+    int s = GPM_OK;
+    cudaStream_t side = dense_stream(&s);
+    if (s != GPM_OK) return s;
     GPM_CUDA(cudaEventRecord(p->fork, st));
-    GPM_CUDA(cudaStreamWaitEvent(p->side, p->fork, 0));
-    k_tc_dense<<<p->dense_grid, 256, p->dense_smem, p->side>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p,
-                                                                p->plong.p, p->dense_tasks.p, p->n_dense,
-                                                                reinterpret_cast<const uint4 *>(p->rows.p),
-                                                                p->counters.p + 2, d_out);
+    GPM_CUDA(cudaStreamWaitEvent(side, p->fork, 0));
+    k_tc_dense<<<p->dense_grid, 256, p->dense_smem, side>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p,
+                                                             p->plong.p, p->dense_tasks.p, p->n_dense,
+                                                             reinterpret_cast<const uint4 *>(p->rows.p),
+                                                             p->counters.p + 2, d_out);
     GPM_LAUNCH_CHECK();
-    GPM_CUDA(cudaEventRecord(p->join, p->side));
+    GPM_CUDA(cudaEventRecord(p->join, side));
   }
   if (rec)
     k_tc_rank_t<true><<<rank_grid(), 256, kRankSmem, st>>>(

@@ -14,19 +14,23 @@ namespace gpm {
 #endif
 constexpr int kRankCtaWords = GPM_RANK_CTA_WORDS;
 #ifndef GPM_RANK_CTA_MIN
-// fixed schedule: owners with more keys than this are CTA tasks (R-MAT 22:
-// 7.65 ms at 50 against 8.0 ms at the reference's USE_CTA = 100 and 7.67 ms
-// at 70; smaller owners rarely fit a warp's bitmap and hash instead)
-#define GPM_RANK_CTA_MIN 50
+// fixed schedule: owners with more keys than this are CTA tasks.  With the
+// dense core segments in their own kernel, R-MAT 20 / 21 / 22 (ms): 100 ->
+// 1.030 / 2.210 / 5.349, 80 -> 1.002 / - / 5.472, 128 -> 1.269 / 2.212 /
+// 5.367, 160 -> 1.349 / 2.800 / 5.370 (long threshold 48); before the dense
+// core the best was 50 (R-MAT 22 6.49 ms, against 6.55 at 128)
+#define GPM_RANK_CTA_MIN 100
 #endif
 constexpr int kRankCtaMin = GPM_RANK_CTA_MIN;
 // fixed schedule: partner segments of at least this many keys are streamed
-// by a half-warp, shorter ones by 4-lane groups (16-byte rows, R-MAT 22:
-// 6.47-6.49 ms at 16, 6.53 at 8, 6.51-6.57 at 24; with 8-lane groups 6.63 ms
-// at 32, 6.66 at 24 and 128, 6.72 at 64; 2-lane groups 6.52 ms at 8 or 16;
-// every segment to 8-lane groups 7.17 ms)
+// by a half-warp, shorter ones by 4-lane groups (16-byte rows).  With the
+// dense core (CTA threshold 100), R-MAT 20 / 21 / 22 (ms): 48 -> 1.030 /
+// 2.210 / 5.349, 64 -> 1.023 / 2.211 / 5.441, 96 -> 1.011 / 2.194 / 5.424,
+// 32 -> 1.048 / - / 5.404 (CTA threshold 80: 24 -> 5.580, 32 -> 5.498, 48 ->
+// 5.472 at R-MAT 22); before the dense core 16 was best (R-MAT 22: 6.47-6.49
+// ms at 16, 6.53 at 8, 6.51-6.57 at 24; every segment to 8-lane groups 7.17)
 #ifndef GPM_RANK_LONG_MIN
-#define GPM_RANK_LONG_MIN 16
+#define GPM_RANK_LONG_MIN 48
 #endif
 constexpr int kRankLongMin = GPM_RANK_LONG_MIN;
 
@@ -92,7 +96,7 @@ __host__ __device__ __forceinline__ int core_clear_words(int32_t kmin, int32_t k
 //               partner's list inside [min N(x), max N(x)] (no key outside
 //               that range can be in N(x)); empty ranges are left out
 //   cta_tasks / warp_tasks  owners by size class, heaviest first
-//   rows        dense core (fixed plan only): ranks [core_base, n) with
+//   rows        dense core: ranks [core_base, n) with
 //               core_base a multiple of 128; row r holds, as row_words bits
 //               from core_base, the core keys of one vertex that has at
 //               least GPM_RANK_CORE_MIN of them.  A long segment
@@ -114,15 +118,15 @@ struct RankPlan {
   DevBuf<int32_t> dense_only;   // owners with dense segments only (in neither task queue)
   int n_dense = 0, n_dense_only = 0, dense_grid = 0;
   size_t dense_smem = 0;
-  // k_tc_dense runs on `side`, forked from and joined back into the caller's
-  // stream by the two events, so that it overlaps the count kernel
-  cudaStream_t side = nullptr;
+  // k_tc_dense runs on the device's side stream (one per device, kept until
+  // exit), forked from and joined back into the caller's stream by the two
+  // events, so that it overlaps the count kernel
   cudaEvent_t fork = nullptr, join = nullptr;
   RankPlan() = default;
   RankPlan(const RankPlan &) = delete;
   RankPlan &operator=(const RankPlan &) = delete;
   ~RankPlan() {
-    if (side) cudaStreamSynchronize(side), cudaStreamDestroy(side);
+    if (join) cudaEventSynchronize(join);  // the side stream's last use of the buffers
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
   }

@@ -129,16 +129,16 @@ def core_words(kmin, kmax):
     return (((kmax - base) >> 5) + 4) & ~3, (((kmax - base + 1) >> 5) + 4) & ~3
 
 
-def plan_numpy(off, idx, core=16384, core_min=128, dense_pct=100, cta_min=50, cta_words=6144):
+def plan_numpy(off, idx, core=16384, core_min=128, dense_pct=100, cta_words=6144):
     """The fixed plan's work restated in numpy: rank by (degree, id), DAG
     edges upward, owner = endpoint with the longer out-list (ties to the
     source), segment = the partner's list clipped to [min, max] of the
     owner's list (owners with fewer than 2 keys have none).  Dense core:
     ranks from core_base = (n - core) rounded down to 128; a vertex with at
-    least core_min keys there has a row; a segment is dense when its owner's
-    keys all lie in the core, its owner's core bitmap fits the owner's queue
-    (cta_words, an eighth for warp tasks), its partner has a row and its keys
-    are at least dense_pct % of the owner's bitmap words.  Returns (segments,
+    least core_min keys there has a row (no rows at all when a row would be
+    wider than cta_words words); a segment is dense when its owner's keys all
+    lie in the core, its partner has a row and its keys are at least
+    dense_pct % of the owner's bitmap words.  Returns (segments,
     keys of the non-dense segments, owner keys, owner tasks, dense segments,
     their words)."""
     n = len(off) - 1
@@ -172,9 +172,8 @@ def plan_numpy(off, idx, core=16384, core_min=128, dense_pct=100, cta_min=50, ct
     rowed = np.bincount(us[vs >= cb], minlength=n) >= max(1, core_min)
     if core > 0 and n > 0 and row_words <= cta_words and rowed.any():
         ko, kx = kmin[owner].astype(np.int64), kmax[owner].astype(np.int64)
-        aw, cw = core_words(ko, kx)
-        nwords = np.where(dp[owner] > cta_min, cta_words, cta_words // 8)
-        dense = seg & (ko >= cb) & rowed[partner] & (cw <= nwords) & (100 * clip >= dense_pct * aw)
+        aw, _ = core_words(ko, kx)
+        dense = seg & (ko >= cb) & rowed[partner] & (100 * clip >= dense_pct * aw)
     return (int(seg.sum()), int(clip[~dense].sum()), int(dp[tasks].sum()), len(tasks), int(dense.sum()),
             int(aw[dense].sum()))
 
