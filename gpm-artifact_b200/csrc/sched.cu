@@ -165,7 +165,7 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
 // room).  One warp per owner; lane 0 writes.
 __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restrict__ roff,
                                                const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                                               const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
+                                               const Seg *__restrict__ pseg, const int32_t *__restrict__ plong,
                                                const int32_t *__restrict__ pshort, unsigned lane, float *f) {
   const int64_t d = roff[x + 1] - roff[x];
   const int nl = plong[x], nseg = nl + pshort[x];
@@ -173,8 +173,7 @@ __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restr
   unsigned long long work = 0;
   long long mx = 0, nlong = 0;
   for (int i = (int)lane; i < nseg; i += 32) {
-    const longlong2 sg = pseg[i < nl ? poff[x] + i : back + i];
-    long long len = sg.x < 0 ? sg.y : sg.y - sg.x;  // a dense segment {-1 - row, keys}
+    const long long len = seg_keys(pseg[i < nl ? poff[x] + i : back + i]);
     work += (unsigned long long)len;
     mx = max(mx, len);
     nlong += len >= 32;
@@ -195,7 +194,7 @@ __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restr
 
 __global__ void k_features(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
                            const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                           const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
+                           const Seg *__restrict__ pseg, const int32_t *__restrict__ plong,
                            const int32_t *__restrict__ pshort, float *__restrict__ X) {
   const unsigned lane = lane_id();
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -221,7 +220,7 @@ __global__ void k_gather_costs(const int32_t *__restrict__ tasks, int ntasks, co
 // otherwise); every task's predicted cost is summed into *total.
 __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ tasks, int ntasks,
                                                 const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                                                const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
+                                                const int64_t *__restrict__ poff, const Seg *__restrict__ pseg,
                                                 const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
                                                 const float *__restrict__ w, uint8_t *__restrict__ cfg,
                                                 float *__restrict__ warp_cost, uint8_t *__restrict__ cta_alt,

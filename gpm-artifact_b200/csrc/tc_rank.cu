@@ -126,7 +126,7 @@ __device__ __forceinline__ unsigned hit4(const T &t, int4 v) {
 // by k_tc_dense and skipped here.
 template <class T>
 __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__restrict__ radj4,
-                                                            const longlong2 *__restrict__ pseg, int64_t l0,
+                                                            const Seg *__restrict__ pseg, int64_t l0,
                                                             int64_t l1, int64_t s0, int64_t s1, const T &t,
                                                             int wid, int nw, unsigned lane) {
   const int4 *__restrict__ rows = reinterpret_cast<const int4 *>(radj4);
@@ -134,9 +134,9 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
   int64_t j;
   const unsigned half = lane >> 4, hl = lane & 15;
   for (j = l0 + wid * 2 + half; j < l1; j += nw * 2) {
-    const longlong2 sg = pseg[j];
-    const int4 *__restrict__ q = rows + (sg.x >> 2);
-    const int nr = sg.x < 0 ? 0 : (int)(((sg.y + 3) >> 2) - (sg.x >> 2));  // dense: none
+    const Seg sg = pseg[j];
+    const int4 *__restrict__ q = rows + max(sg.x, 0);
+    const int nr = sg.x < 0 ? 0 : seg_rows(sg);  // dense: none
     unsigned cs = 0;
 #pragma unroll kRankUnroll
     for (int i = (int)hl; i < nr; i += 16) cs += hit4(t, __ldg(q + i));
@@ -145,9 +145,10 @@ __device__ __forceinline__ unsigned long long scan_segments(const int32_t *__res
   constexpr int S = GPM_RANK_SHORT_LANES, G = 32 / S;
   const unsigned grp = lane / S, gl = lane % S;
   for (j = s0 + wid * G + grp; j < s1; j += nw * G) {
-    const longlong2 sg = pseg[j];
+    const Seg sg = pseg[j];
     unsigned cs = 0;
-    for (int64_t k = (sg.x >> 2) + gl; k < (sg.y + 3) >> 2; k += S) cs += hit4(t, __ldg(rows + k));
+    const int64_t k1 = (int64_t)sg.x + seg_rows(sg);
+    for (int64_t k = (int64_t)sg.x + gl; k < k1; k += S) cs += hit4(t, __ldg(rows + k));
     c += cs;
   }
   return c;
@@ -175,7 +176,7 @@ __device__ __forceinline__ unsigned long long owner_task(int32_t x, const int64_
                                                          const int32_t *__restrict__ radj,
                                                          const int32_t *__restrict__ radj4,
                                                          const int64_t *__restrict__ poff,
-                                                         const longlong2 *__restrict__ pseg,
+                                                         const Seg *__restrict__ pseg,
                                                          const int32_t *__restrict__ plong,
                                                          const int32_t *__restrict__ pshort, uint32_t *words,
                                                          int nwords, unsigned long long *rec) {
@@ -245,7 +246,7 @@ template <bool REC>
 __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
     k_tc_rank_t(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
                 const int32_t *__restrict__ radj4, const int64_t *__restrict__ poff,
-                const longlong2 *__restrict__ pseg,
+                const Seg *__restrict__ pseg,
                 const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
                 const int32_t *__restrict__ cta_tasks, int n_cta,
                 const int32_t *__restrict__ warp_tasks, int n_warp, int *__restrict__ counters,
@@ -303,7 +304,7 @@ constexpr int kDenseLanes = GPM_RANK_DENSE_LANES;
 constexpr int kDenseUnroll = GPM_RANK_DENSE_UNROLL;
 __global__ void __launch_bounds__(256, 4)
     k_tc_dense(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-               const longlong2 *__restrict__ pseg, const int32_t *__restrict__ plong,
+               const Seg *__restrict__ pseg, const int32_t *__restrict__ plong,
                const int32_t *__restrict__ tasks, int ntasks, const uint4 *__restrict__ rows4,
                int *__restrict__ counter, unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t dsm[];
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(256, 4)
     __syncthreads();
     const int64_t l0 = poff[x], l1 = l0 + plong[x];
     for (int64_t j = l0 + grp; j < l1; j += ngrp) {
-      const int64_t sx = pseg[j].x;
+      const int sx = pseg[j].x;
       if (sx >= 0) continue;
       const uint4 *__restrict__ r = rows4 + (-1 - sx);
       unsigned cs = 0;
@@ -517,10 +518,10 @@ __global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, con
                                 const int64_t *__restrict__ roff4, int32_t *__restrict__ radj4, int upward,
                                 int long_min, const uint8_t *__restrict__ cfg,
                                 const int64_t *__restrict__ poff, int32_t *__restrict__ plong,
-                                int32_t *__restrict__ pshort, longlong2 *__restrict__ pseg,
+                                int32_t *__restrict__ pshort, Seg *__restrict__ pseg,
                                 unsigned long long *__restrict__ work, int32_t core_base,
                                 const int32_t *__restrict__ rowid, int row_words, int dense_pct,
-                                int32_t *__restrict__ pdense) {
+                                int32_t *__restrict__ pdense, int *__restrict__ too_long) {
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t u = warp; u < n; u += nw) {
@@ -566,7 +567,9 @@ __global__ void k_partner_place(int64_t n, const int64_t *__restrict__ roff, con
       const int64_t slot = grp.shfl(base, 0) + (int64_t)grp.thread_rank();
       const int64_t pos = lng ? poff[owner] + slot : poff[owner + 1] - 1 - slot;
       const int64_t lo4 = lo - roff[partner] + roff4[partner];  // the same keys in radj4
-      pseg[pos] = row >= 0 ? make_longlong2(-1 - row, len) : make_longlong2(lo4, lo4 + len);
+      if (len >= (1 << 29)) *too_long = 1;  // no 8-byte descriptor for it
+      pseg[pos] = row >= 0 ? make_int2((int)(-1 - row), (int)(len << 2))
+                           : make_int2((int)(lo4 >> 2), (int)((len << 2) | (lo4 & 3)));
       const unsigned long long w = cg::reduce(grp, (unsigned long long)units + 1ull, cg::plus<unsigned long long>());
       if (grp.thread_rank() == 0) atomicAdd(&work[owner], w);
       if (rowid) {
@@ -1149,18 +1152,26 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
   cudaMemsetAsync(p->plong.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(p->pshort.p, 0, sizeof(int32_t) * n, st);
   cudaMemsetAsync(work.p, 0, sizeof(unsigned long long) * n, st);
+  // 8-byte segment descriptors address radj4 by 16-byte rows in 31 bits
+  if ((int64_t)(g->rg->radj4.n / 4) >= ((int64_t)1 << 31))
+    return bail(fail(GPM_EUNSUPPORTED, "triangle plan: more than 2^33 padded keys"));
   DevBuf<int32_t> rowid;
   int dense_pct = 0;
   // the dense core does not depend on the schedule: every plan has it
-  GPM_TRY(build_core_rows(g, p, rowid, &dense_pct, st));
+  if ((s = build_core_rows(g, p, rowid, &dense_pct, st))) return bail(s);
   if (p->n_rows) {
-    GPM_TRY(p->pdense.reserve(n));
-    GPM_CUDA(cudaMemsetAsync(p->pdense.p, 0, sizeof(int32_t) * n, st));
+    if ((s = p->pdense.reserve(n))) return bail(s);
+    cudaMemsetAsync(p->pdense.p, 0, sizeof(int32_t) * n, st);
   }
+  // sizes: [0] CTA tasks, [1] warp tasks, [2] dense tasks, [3] dense-only
+  // owners, [4] a segment too long for its descriptor
+  DevBuf<int> sizes;
+  if ((s = sizes.reserve(5))) return bail(s);
+  cudaMemsetAsync(sizes.p, 0, 5 * sizeof(int), st);
   k_partner_place<<<grid_for(n * 32), 256, 0, st>>>(n, roff, radj, g->rg->roff4.p, fill ? g->rg->radj4.p : nullptr,
                                                      g->rg->upward, long_min, cfg, p->poff.p, p->plong.p, p->pshort.p,
                                                      p->pseg.p, work.p, p->core_base, p->n_rows ? rowid.p : nullptr,
-                                                     p->row_words, dense_pct, p->pdense.p);
+                                                     p->row_words, dense_pct, p->pdense.p, sizes.p + 4);
   GPM_LAUNCH_CHECK();
   if (fill) g->rg->padded = 1;
   // 3. task queues, heaviest first
@@ -1168,11 +1179,9 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
   DevBuf<int32_t> cval, wval;
   DevBuf<unsigned long long> dkey;
   DevBuf<int32_t> dval;
-  DevBuf<int> sizes;
   if ((s = ckey.reserve(n)) || (s = wkey.reserve(n)) || (s = cval.reserve(n)) || (s = wval.reserve(n)) ||
-      (s = sizes.reserve(4)) || (s = p->cta_tasks.reserve(n)) || (s = p->warp_tasks.reserve(n)))
+      (s = p->cta_tasks.reserve(n)) || (s = p->warp_tasks.reserve(n)))
     return bail(s);
-  cudaMemsetAsync(sizes.p, 0, 4 * sizeof(int), st);
   const int32_t *pdense = p->n_rows ? p->pdense.p : nullptr;
   if (pdense && (s = p->dense_only.reserve(n))) return bail(s);
   k_rank_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, p->plong.p, p->pshort.p, work.p, cta_min, cfg, pdense,
@@ -1181,10 +1190,11 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
     if ((s = dkey.reserve(n)) || (s = dval.reserve(n))) return bail(s);
     k_dense_tasks<<<grid_for(n), 256, 0, st>>>(n, roff, radj, pdense, dkey.p, dval.p, sizes.p + 2);
   }
-  int h[4] = {0, 0, 0, 0};
+  int h[5] = {0, 0, 0, 0, 0};
   cudaMemcpyAsync(h, sizes.p, sizeof h, cudaMemcpyDeviceToHost, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank plan: ") + cudaGetErrorString(e)));
+  if (h[4]) return bail(fail(GPM_EUNSUPPORTED, "triangle plan: a partner segment of 2^29 keys or more"));
   p->n_cta = h[0];
   p->n_warp = h[1];
   p->n_dense = h[2];
@@ -1259,7 +1269,7 @@ int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
 
 // out[0] segments, out[1] keys in them, out[2] keys of the owners' lists
 __global__ void k_plan_stats(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
-                             const int64_t *__restrict__ poff, const longlong2 *__restrict__ pseg,
+                             const int64_t *__restrict__ poff, const Seg *__restrict__ pseg,
                              const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
                              const int32_t *__restrict__ radj, unsigned long long *__restrict__ out) {
   unsigned long long segs = 0, keys = 0, okeys = 0, dsegs = 0, dwords = 0;
@@ -1272,11 +1282,10 @@ __global__ void k_plan_stats(const int32_t *__restrict__ tasks, int ntasks, cons
         ++dsegs;
         dwords += (unsigned long long)core_and_words(radj[roff[x]], radj[roff[x + 1] - 1]);
       } else {
-        keys += (unsigned long long)(pseg[j].y - pseg[j].x);
+        keys += (unsigned long long)seg_keys(pseg[j]);
       }
     }
-    for (int64_t j = poff[x + 1] - pshort[x]; j < poff[x + 1]; ++j)
-      keys += (unsigned long long)(pseg[j].y - pseg[j].x);
+    for (int64_t j = poff[x + 1] - pshort[x]; j < poff[x + 1]; ++j) keys += (unsigned long long)seg_keys(pseg[j]);
   }
   segs = warp_sum(segs);
   keys = warp_sum(keys);

@@ -74,6 +74,15 @@ struct RankGraph {
 #define GPM_RANK_DENSE_PCT 100
 #endif
 
+// A partner segment in 8 bytes.  A segment read as keys: x = its first
+// 16-byte row of radj4 (>= 0), y = keys << 2 | the position of its first key
+// in that row; dense: x = -1 - (uint4 index of its core row words), y =
+// keys << 2.  Plans stop with GPM_EUNSUPPORTED where radj4 holds 2^31 rows or
+// more, or a segment 2^29 keys or more.
+using Seg = int2;
+__host__ __device__ __forceinline__ int seg_keys(Seg s) { return (int)((uint32_t)s.y >> 2); }
+__host__ __device__ __forceinline__ int seg_rows(Seg s) { return (int)(((s.y & 3) + ((uint32_t)s.y >> 2) + 3) >> 2); }
+
 // Core bitmaps of an owner x whose keys all lie in the core (min N(x) >=
 // core_base): N(x) as bits from base = min N(x) rounded down to 128, so
 // bitmap word i lines up with word (base - core_base) / 32 + i of every core
@@ -131,7 +140,7 @@ struct RankPlan {
     if (join) cudaEventDestroy(join);
   }
   DevBuf<int64_t> poff;
-  DevBuf<longlong2> pseg;
+  DevBuf<Seg> pseg;
   DevBuf<int32_t> plong, pshort;
   DevBuf<int32_t> cta_tasks, warp_tasks;
   DevBuf<int> counters;
