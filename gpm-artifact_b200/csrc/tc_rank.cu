@@ -1101,7 +1101,9 @@ static int build_core_rows(gpm_graph *g, RankPlan *p, DevBuf<int32_t> &rowid, in
   if (K <= 0 || n <= 0 || n > INT32_MAX - 128) return GPM_OK;
   const int32_t core_base = (int32_t)(std::max<int64_t>(0, n - K) & ~(int64_t)127);
   const int64_t row_words = ((n - core_base + 127) >> 7) << 2;
-  if (row_words > (int64_t)kRankCtaWords) return GPM_OK;  // wider than any owner bitmap
+  // k_tc_dense holds an owner's bitmap of up to row_words + 4 words in shared
+  // memory, sized (and its occupancy taken) for kRankCtaWords + 4
+  if (row_words > (int64_t)kRankCtaWords) return GPM_OK;
   DevBuf<int> nrows;
   GPM_TRY(rowid.reserve(n));
   GPM_TRY(nrows.reserve(1));
@@ -1115,6 +1117,7 @@ static int build_core_rows(gpm_graph *g, RankPlan *p, DevBuf<int32_t> &rowid, in
   if (h <= 0) return GPM_OK;
   const size_t bytes = (size_t)h * (size_t)row_words * 4;
   if (bytes > std::max<size_t>((size_t)1 << 30, 16 * (size_t)g->rg->radj.n)) return GPM_OK;
+  if (bytes / 16 >= ((size_t)1 << 31)) return GPM_OK;  // a dense descriptor indexes the rows' uint4 in 31 bits
   GPM_TRY(p->rows.reserve((size_t)h * (size_t)row_words));
   GPM_CUDA(cudaMemsetAsync(p->rows.p, 0, bytes, st));
   k_core_rows<<<grid_for(n * 32), 256, 0, st>>>(n, g->rg->roff.p, g->rg->radj.p, core_base, rowid.p,
