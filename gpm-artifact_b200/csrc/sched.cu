@@ -160,20 +160,39 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
 }
 
 // ------------------------------------------------------------ features
+// The partner segments of a plan: owner x's long ones at pseg[poff[x] ..
+// + plong[x]), its short ones at the back of its room (pshort[x] of them,
+// ending at poff[x+1]), its dense ones (plans with a dense core) at
+// dseg[doff[x] .. doff[x+1]).
+struct SegView {
+  const int64_t *poff;
+  const Seg *pseg;
+  const int32_t *plong, *pshort;
+  const int64_t *doff;  // nullptr: no dense segments
+  const Seg *dseg;
+};
+static SegView seg_view(const RankPlan *h) {
+  return SegView{h->poff.p, h->pseg.p, h->plong.p, h->pshort.p, h->n_rows ? h->doff.p : nullptr,
+                 h->n_rows ? h->dseg.p : nullptr};
+}
+
 // Owner x (a task of the heuristic plan): 8 features from its key list and
-// its partner segments (the front plong[x] and back pshort[x] slots of its
-// room).  One warp per owner; lane 0 writes.
+// all its partner segments (long, dense and short alike).  One warp per
+// owner; lane 0 writes.
 __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restrict__ roff,
-                                               const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                                               const Seg *__restrict__ pseg, const int32_t *__restrict__ plong,
-                                               const int32_t *__restrict__ pshort, unsigned lane, float *f) {
+                                               const int32_t *__restrict__ radj, const SegView &v, unsigned lane,
+                                               float *f) {
   const int64_t d = roff[x + 1] - roff[x];
-  const int nl = plong[x], nseg = nl + pshort[x];
-  const int64_t back = poff[x + 1] - pshort[x] - nl;  // slot i >= nl lives at back + i
+  const int nl = v.plong[x], ns = v.pshort[x];
+  const int64_t d0 = v.doff ? v.doff[x] : 0;
+  const int nd = v.doff ? (int)(v.doff[x + 1] - d0) : 0;
+  const int nseg = nl + nd + ns;
+  const int64_t back = v.poff[x + 1] - ns - nl - nd;  // short slot i >= nl + nd lives at back + i
   unsigned long long work = 0;
   long long mx = 0, nlong = 0;
   for (int i = (int)lane; i < nseg; i += 32) {
-    const long long len = seg_keys(pseg[i < nl ? poff[x] + i : back + i]);
+    const Seg sg = i < nl ? v.pseg[v.poff[x] + i] : i < nl + nd ? v.dseg[d0 + (i - nl)] : v.pseg[back + i];
+    const long long len = seg_keys(sg);
     work += (unsigned long long)len;
     mx = max(mx, len);
     nlong += len >= 32;
@@ -193,15 +212,13 @@ __device__ __forceinline__ void owner_features(int32_t x, const int64_t *__restr
 }
 
 __global__ void k_features(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
-                           const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-                           const Seg *__restrict__ pseg, const int32_t *__restrict__ plong,
-                           const int32_t *__restrict__ pshort, float *__restrict__ X) {
+                           const int32_t *__restrict__ radj, SegView v, float *__restrict__ X) {
   const unsigned lane = lane_id();
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t t = warp; t < ntasks; t += nw) {
     float f[kIn];
-    owner_features(tasks[t], roff, radj, poff, pseg, plong, pshort, lane, f);
+    owner_features(tasks[t], roff, radj, v, lane, f);
     if (lane == 0)
       for (int i = 0; i < kIn; ++i) X[t * kIn + i] = f[i];
   }
@@ -220,9 +237,7 @@ __global__ void k_gather_costs(const int32_t *__restrict__ tasks, int ntasks, co
 // otherwise); every task's predicted cost is summed into *total.
 __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ tasks, int ntasks,
                                                 const int64_t *__restrict__ roff, const int32_t *__restrict__ radj,
-                                                const int64_t *__restrict__ poff, const Seg *__restrict__ pseg,
-                                                const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
-                                                const float *__restrict__ w, uint8_t *__restrict__ cfg,
+                                                SegView v, const float *__restrict__ w, uint8_t *__restrict__ cfg,
                                                 float *__restrict__ warp_cost, uint8_t *__restrict__ cta_alt,
                                                 double *__restrict__ total) {
   __shared__ float sw[kParams];
@@ -235,7 +250,7 @@ __global__ void __launch_bounds__(256) k_assign(const int32_t *__restrict__ task
   for (int64_t t = warp; t < ntasks; t += nw) {
     float f[kIn];
     const int32_t x = tasks[t];
-    owner_features(x, roff, radj, poff, pseg, plong, pshort, lane, f);
+    owner_features(x, roff, radj, v, lane, f);
     if (lane == 0) {
       float h1[kH], h2[kH], y[kOut];
       mlp_forward(sw, f, h1, h2, y);
@@ -304,9 +319,8 @@ static int assign_configs(gpm_graph *g, gpm_sched *s, const int32_t *tasks, int 
   GPM_TRY(total.reserve(1));
   GPM_CUDA(cudaMemsetAsync(total.p, 0, sizeof(double), st));
   RankPlan *h = g->rank;
-  k_assign<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p, h->pseg.p,
-                                                     h->plong.p, h->pshort.p, s->w.p, cfg, warp_cost.p, cta_alt.p,
-                                                     total.p);
+  k_assign<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks, nt, g->rg->roff.p, g->rg->radj.p, seg_view(h), s->w.p,
+                                                     cfg, warp_cost.p, cta_alt.p, total.p);
   GPM_LAUNCH_CHECK();
   // warp slots of the count kernel: 8 CTAs of 8 warps per SM
   k_rail<<<blocks(nt), 256, 0, st>>>(tasks, nt, warp_cost.p, cta_alt.p, total.p, 64.0 * num_sms(), cfg);
@@ -438,8 +452,8 @@ int gpm_sched_collect(gpm_sched *s, gpm_graph *g, int64_t *rows_added) {
     s->cap = cap;
   }
   RankPlan *h = g->rank;
-  k_features<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, h->poff.p,
-                                                       h->pseg.p, h->plong.p, h->pshort.p, s->X.p + s->rows * kIn);
+  k_features<<<blocks((int64_t)nt * 32), 256, 0, st>>>(tasks.p, nt, g->rg->roff.p, g->rg->radj.p, seg_view(h),
+                                                       s->X.p + s->rows * kIn);
   DevBuf<unsigned long long> rec, cnt;
   DevBuf<uint8_t> cfg;
   GPM_TRY(rec.reserve(g->n));

@@ -283,8 +283,8 @@ __global__ void __launch_bounds__(256, GPM_TC_RANK_MIN_BLOCKS)
 
 // Dense segments of the core owners, one owner per CTA task (heaviest
 // first): N(x) as a bitmap from base = min N(x) rounded down to 128 in shared
-// memory (core_clear_words, at most row_words + 4), then every dense long
-// segment {-1 - i, keys} of x by a group of kDenseLanes lanes: the partner's
+// memory (core_clear_words, at most row_words + 4), then every dense
+// segment {-1 - i, keys} of x (dseg[doff[x] .. doff[x+1])) by a group of kDenseLanes lanes: the partner's
 // core row words from base on (rows4[i] ..), ANDed 16 bytes per lane with the
 // bitmap over core_and_words(x) / 4 loads.  Its own launch, so that its
 // register budget (64 at 4 CTAs of 256 per SM) allows several 16-byte loads
@@ -303,10 +303,9 @@ constexpr int kDenseLanes = GPM_RANK_DENSE_LANES;
 #endif
 constexpr int kDenseUnroll = GPM_RANK_DENSE_UNROLL;
 __global__ void __launch_bounds__(256, 4)
-    k_tc_dense(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj, const int64_t *__restrict__ poff,
-               const Seg *__restrict__ pseg, const int32_t *__restrict__ plong,
-               const int32_t *__restrict__ tasks, int ntasks, const uint4 *__restrict__ rows4,
-               int *__restrict__ counter, unsigned long long *__restrict__ out) {
+    k_tc_dense(const int64_t *__restrict__ roff, const int32_t *__restrict__ radj, const int64_t *__restrict__ doff,
+               const Seg *__restrict__ dseg, const int32_t *__restrict__ tasks, int ntasks,
+               const uint4 *__restrict__ rows4, int *__restrict__ counter, unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t dsm[];
   __shared__ int s_task;
   const int grp = threadIdx.x / kDenseLanes, gl = threadIdx.x % kDenseLanes, ngrp = blockDim.x / kDenseLanes;
@@ -329,11 +328,9 @@ __global__ void __launch_bounds__(256, 4)
       atomicOr(&dsm[o >> 5], 1u << (o & 31));
     }
     __syncthreads();
-    const int64_t l0 = poff[x], l1 = l0 + plong[x];
-    for (int64_t j = l0 + grp; j < l1; j += ngrp) {
-      const int sx = pseg[j].x;
-      if (sx >= 0) continue;
-      const uint4 *__restrict__ r = rows4 + (-1 - sx);
+    const int64_t d1 = doff[x + 1];
+    for (int64_t j = doff[x] + grp; j < d1; j += ngrp) {
+      const uint4 *__restrict__ r = rows4 + (-1 - dseg[j].x);
       unsigned cs = 0;
 #pragma unroll kDenseUnroll
       for (int i = gl; i < nq; i += kDenseLanes) {
@@ -607,6 +604,41 @@ __global__ void k_core_rows(int64_t n, const int64_t *__restrict__ roff, const i
   }
 }
 
+// The dense segments of owner x (pdense[x] > 0, one warp each) moved out of
+// its long segments into dseg[doff[x] ..); the others closed up at the
+// front of the long region and plong[x] set to their number.  A chunk of 32
+// is read whole before any lane writes, and a write never passes the chunk.
+__global__ void k_split_dense(int64_t n, const int64_t *__restrict__ poff, int32_t *__restrict__ plong,
+                              const int32_t *__restrict__ pdense, const int64_t *__restrict__ doff,
+                              Seg *__restrict__ pseg, Seg *__restrict__ dseg) {
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lane = lane_id(), below = (1u << lane) - 1u;
+  for (int64_t x = warp; x < n; x += nw) {
+    if (pdense[x] == 0) continue;
+    Seg *lg = pseg + poff[x];
+    const int nl = plong[x];
+    int64_t wd = doff[x];
+    int wn = 0;
+    for (int b = 0; b < nl; b += 32) {
+      const bool valid = b + (int)lane < nl;
+      const Seg sg = valid ? lg[b + lane] : make_int2(0, 0);
+      const bool dense = valid && sg.x < 0;
+      const unsigned md = __ballot_sync(0xffffffffu, dense), mn = __ballot_sync(0xffffffffu, valid && !dense);
+      if (dense) dseg[wd + __popc(md & below)] = sg;
+      if (valid && !dense) lg[wn + __popc(mn & below)] = sg;
+      wd += __popc(md);
+      wn += __popc(mn);
+      __syncwarp();
+    }
+    if (lane == 0) plong[x] = wn;
+  }
+}
+__global__ void k_widen(int64_t n, const int32_t *__restrict__ a, int64_t *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
 // roff4: list lengths rounded up to a multiple of four, for the scan that
 // places every list of radj4 at a multiple of four keys
 __global__ void k_padded_len(int64_t n, const int64_t *__restrict__ roff, int64_t *__restrict__ len4) {
@@ -635,9 +667,8 @@ __global__ void k_rank_tasks(int64_t n, const int64_t *__restrict__ roff, const 
                              int32_t *__restrict__ cval, unsigned long long *__restrict__ wkey,
                              int32_t *__restrict__ wval, int *__restrict__ sizes) {
   for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
-    const int nd = pdense ? pdense[x] : 0;
-    if (plong[x] + pshort[x] == nd) {  // nothing left to stream
-      if (nd) donly[atomicAdd(&sizes[3], 1)] = (int32_t)x;  // dense segments only
+    if (plong[x] + pshort[x] == 0) {  // nothing to stream
+      if (pdense && pdense[x]) donly[atomicAdd(&sizes[3], 1)] = (int32_t)x;  // dense segments only
       continue;
     }
     int64_t d = roff[x + 1] - roff[x];
@@ -1176,6 +1207,20 @@ int rank_plan_new(gpm_graph *g, int cta_min, int long_min, const uint8_t *cfg, c
                                                      p->pseg.p, work.p, p->core_base, p->n_rows ? rowid.p : nullptr,
                                                      p->row_words, dense_pct, p->pdense.p, sizes.p + 4);
   GPM_LAUNCH_CHECK();
+  if (p->n_rows) {  // the dense segments moved out of the long ones
+    DevBuf<int64_t> cnt;
+    if ((s = cnt.reserve(n)) || (s = p->doff.reserve(n + 1))) return bail(s);
+    k_widen<<<grid_for(n), 256, 0, st>>>(n, p->pdense.p, cnt.p);
+    if ((s = scan_i64(n, cnt.p, p->doff.p, st))) return bail(s);
+    int64_t total = 0;
+    cudaMemcpyAsync(&total, p->doff.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    cudaError_t e0 = cudaStreamSynchronize(st);
+    if (e0 != cudaSuccess) return bail(fail(GPM_ECUDA, std::string("rank plan: ") + cudaGetErrorString(e0)));
+    if ((s = p->dseg.reserve(std::max<int64_t>(total, 1)))) return bail(s);
+    k_split_dense<<<grid_for(n * 32), 256, 0, st>>>(n, p->poff.p, p->plong.p, p->pdense.p, p->doff.p, p->pseg.p,
+                                                    p->dseg.p);
+    GPM_LAUNCH_CHECK();
+  }
   if (fill) g->rg->padded = 1;
   // 3. task queues, heaviest first
   DevBuf<unsigned long long> ckey, wkey;
@@ -1242,8 +1287,8 @@ int rank_plan_launch(gpm_graph *g, RankPlan *p, cudaStream_t st, unsigned long l
     if (s != GPM_OK) return s;
     GPM_CUDA(cudaEventRecord(p->fork, st));
     GPM_CUDA(cudaStreamWaitEvent(side, p->fork, 0));
-    k_tc_dense<<<p->dense_grid, 256, p->dense_smem, side>>>(g->rg->roff.p, g->rg->radj.p, p->poff.p, p->pseg.p,
-                                                             p->plong.p, p->dense_tasks.p, p->n_dense,
+    k_tc_dense<<<p->dense_grid, 256, p->dense_smem, side>>>(g->rg->roff.p, g->rg->radj.p, p->doff.p, p->dseg.p,
+                                                             p->dense_tasks.p, p->n_dense,
                                                              reinterpret_cast<const uint4 *>(p->rows.p),
                                                              p->counters.p + 2, d_out);
     GPM_LAUNCH_CHECK();
@@ -1274,20 +1319,19 @@ int rank_launch(gpm_graph *g, cudaStream_t st, unsigned long long *d_out) {
 __global__ void k_plan_stats(const int32_t *__restrict__ tasks, int ntasks, const int64_t *__restrict__ roff,
                              const int64_t *__restrict__ poff, const Seg *__restrict__ pseg,
                              const int32_t *__restrict__ plong, const int32_t *__restrict__ pshort,
-                             const int32_t *__restrict__ radj, unsigned long long *__restrict__ out) {
+                             const int32_t *__restrict__ pdense, const int32_t *__restrict__ radj,
+                             unsigned long long *__restrict__ out) {
   unsigned long long segs = 0, keys = 0, okeys = 0, dsegs = 0, dwords = 0;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntasks; t += (int64_t)gridDim.x * blockDim.x) {
     const int32_t x = tasks[t];
+    const int nd = pdense ? pdense[x] : 0;
     okeys += (unsigned long long)(roff[x + 1] - roff[x]);
-    segs += (unsigned long long)(plong[x] + pshort[x]);
-    for (int64_t j = poff[x]; j < poff[x] + plong[x]; ++j) {
-      if (pseg[j].x < 0) {  // dense: the owner's bitmap words
-        ++dsegs;
-        dwords += (unsigned long long)core_and_words(radj[roff[x]], radj[roff[x + 1] - 1]);
-      } else {
-        keys += (unsigned long long)seg_keys(pseg[j]);
-      }
+    segs += (unsigned long long)(plong[x] + pshort[x] + nd);
+    if (nd) {  // dense: the owner's bitmap words each
+      dsegs += (unsigned long long)nd;
+      dwords += (unsigned long long)nd * (unsigned long long)core_and_words(radj[roff[x]], radj[roff[x + 1] - 1]);
     }
+    for (int64_t j = poff[x]; j < poff[x] + plong[x]; ++j) keys += (unsigned long long)seg_keys(pseg[j]);
     for (int64_t j = poff[x + 1] - pshort[x]; j < poff[x + 1]; ++j) keys += (unsigned long long)seg_keys(pseg[j]);
   }
   segs = warp_sum(segs);
@@ -1313,13 +1357,14 @@ int rank_plan_stats(gpm_graph *g, uint64_t *out) {
   GPM_TRY(o.reserve(5));
   GPM_CUDA(cudaMemset(o.p, 0, 40));
   const int grid = num_sms() * 8;
+  const int32_t *pdense = p->n_rows ? p->pdense.p : nullptr;
   k_plan_stats<<<grid, 256>>>(p->cta_tasks.p, p->n_cta, g->rg->roff.p, p->poff.p, p->pseg.p, p->plong.p,
-                              p->pshort.p, g->rg->radj.p, o.p);
+                              p->pshort.p, pdense, g->rg->radj.p, o.p);
   k_plan_stats<<<grid, 256>>>(p->warp_tasks.p, p->n_warp, g->rg->roff.p, p->poff.p, p->pseg.p, p->plong.p,
-                              p->pshort.p, g->rg->radj.p, o.p);
+                              p->pshort.p, pdense, g->rg->radj.p, o.p);
   if (p->n_dense_only)
     k_plan_stats<<<grid, 256>>>(p->dense_only.p, p->n_dense_only, g->rg->roff.p, p->poff.p, p->pseg.p, p->plong.p,
-                                p->pshort.p, g->rg->radj.p, o.p);
+                                p->pshort.p, pdense, g->rg->radj.p, o.p);
   GPM_LAUNCH_CHECK();
   unsigned long long h[5];
   GPM_CUDA(cudaMemcpy(h, o.p, sizeof h, cudaMemcpyDeviceToHost));

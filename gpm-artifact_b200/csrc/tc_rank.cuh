@@ -113,8 +113,8 @@ __host__ __device__ __forceinline__ int core_clear_words(int32_t kmin, int32_t k
 //               count is popc(row & N(owner)) over the owner's words, with
 //               the partner's row words from the owner's base on starting at
 //               uint4 index i of rows, instead of streaming the partner's
-//               keys; k_tc_dense counts these (tasks: dense_tasks) and the
-//               count kernel skips them
+//               keys; placed among the long segments, then moved to dseg
+//               (below); k_tc_dense counts them (tasks: dense_tasks)
 struct RankPlan {
   int cta_min = 0, long_min = 0;
   int n_cta = 0, n_warp = 0;
@@ -123,6 +123,10 @@ struct RankPlan {
   int64_t n_rows = 0;
   DevBuf<uint32_t> rows;
   DevBuf<int32_t> pdense;       // dense segments per owner
+  // the dense segments, apart from pseg: owner x's are dseg[doff[x] ..
+  // doff[x+1]); plong[x] counts only x's other long segments
+  DevBuf<int64_t> doff;         // n + 1
+  DevBuf<Seg> dseg;
   DevBuf<int32_t> dense_tasks;  // owners with dense segments, most words first
   DevBuf<int32_t> dense_only;   // owners with dense segments only (in neither task queue)
   int n_dense = 0, n_dense_only = 0, dense_grid = 0;
