@@ -1,7 +1,7 @@
 // tc_rank.cu -- the B200 triangle-count path (variant GPM_TC_BITMAP).
 //
 // Same sum as every TCSolver variant, T = sum over stored u->v of
-// |N(u) & N(v)|, reorganised four ways:
+// |N(u) & N(v)|, reorganised five ways:
 //
 // 1. Rank relabel.  Vertices are renumbered by (in+out degree, id), the
 //    order the degree orientation (graph.h:128-129) is built on, so a DAG

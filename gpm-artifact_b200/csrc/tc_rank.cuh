@@ -100,10 +100,10 @@ __host__ __device__ __forceinline__ int core_clear_words(int32_t kmin, int32_t k
 //   poff/pseg   partner segments: owner x has the room pseg[poff[x] ..
 //               poff[x+1]) (poff = rinc, one slot per incident edge); its
 //               plong[x] long segments fill the room from the front, its
-//               pshort[x] short ones from the back.  A segment is the
-//               [start, end) range of radj4 holding the part of one
-//               partner's list inside [min N(x), max N(x)] (no key outside
-//               that range can be in N(x)); empty ranges are left out
+//               pshort[x] short ones from the back.  A segment (a Seg,
+//               above) names the 16-byte rows of radj4 holding the part of
+//               one partner's list inside [min N(x), max N(x)] (no key
+//               outside that range can be in N(x)); empty ranges are left out
 //   cta_tasks / warp_tasks  owners by size class, heaviest first
 //   rows        dense core: ranks [core_base, n) with
 //               core_base a multiple of 128; row r holds, as row_words bits
